@@ -1,0 +1,348 @@
+"""Benchmark of the multislice hot path: probe.slice steps/s on the STEM HAADF+BF scan workload.
+
+Workload (the headline STEM configuration): cubic SrTiO3 (a = 3.905 A; Sr at 0, Ti at the body centre, O at the face
+centres) tiled 8 x 8 x 20 (31.24 x 31.24 x 78.1 A, 6,400 atoms), 512 x 512 grid, 20 slices of 3.905 A, Lobato
+infinite-projection potential, 200 keV probe of 20 mrad semiangle with C10 = C30 = 0, a 64 x 64 GridScan over one
+central unit cell (start (4a, 4a), end (5a, 5a), endpoint false), annular detectors BF 0-20 mrad and HAADF 50-200 mrad.
+One bench step = the whole scan: 4,096 positions x 20 slices = 81,920 probe.slice steps. Synthetic structure, no dataset.
+
+Timed region (`value`): `simk_scan_device` with the potential's transmissions already on the device, positions and
+detector outputs on the device; K scans between CUDA events on the library's stream (torch's current stream),
+synchronised and barriered on both sides, max over ranks. The waves of a batch (up to 1 GiB) exceed L2 (126 MB), so
+no flush is needed between steps. `e2e`: the public `STEM.scan` call from host arrays (structure -> potential built on
+the device -> scan -> detector images back to the host), wall-clocked per call.
+
+`--impl reference`: the reference's CPU path (restated in float64 NumPy, oracle/simk_oracle.py; the Swift original
+cannot build on Linux) timed on the host cores on a bounded sample of positions of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+A0 = 3.905
+NX = NY = 512
+SLICE = 3.905
+ENERGY = 200e3
+SEMIANGLE = 20.0
+SCAN_N = 64
+DETECTORS = [("BF", 0.0, 20.0), ("HAADF", 50.0, 200.0)]
+WORKLOAD = "STEM HAADF+BF scan, SrTiO3 8x8x20 (6400 atoms, 78.1 A), 512x512, 20 slices of 3.905 A, 200 keV, " \
+           "20 mrad, 64x64 scan over one unit cell"
+
+
+def srtio3(nx, ny, nz):
+    frac = np.array([(0, 0, 0), (0.5, 0.5, 0.5), (0.5, 0.5, 0), (0.5, 0, 0.5), (0, 0.5, 0.5)], dtype=np.float64)
+    nums = np.array([38, 22, 8, 8, 8])
+    shifts = np.array([(i, j, k) for i in range(nx) for j in range(ny) for k in range(nz)], dtype=np.float64)
+    pos = ((shifts[:, None, :] + frac[None, :, :]) * A0).reshape(-1, 3)
+    return (nx * A0, ny * A0, nz * A0), np.tile(nums, len(shifts)), pos
+
+
+def scan_positions():
+    xs = np.arange(SCAN_N) * (A0 / SCAN_N) + 4 * A0
+    return np.stack(np.meshgrid(xs, xs, indexing="ij"), axis=-1).reshape(-1, 2)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def traffic_from_profiles(kernel: str):
+    """dram bytes per launch of `kernel` on this workload from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        v = d.get(kernel)
+        if isinstance(v, dict):
+            return v.get("dram_bytes_per_launch")
+    return None
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# CPU: the reference's path restated (oracle), on host threads over positions
+# ---------------------------------------------------------------------------------------------------------------------
+
+def cpu_reference(n_positions: int, threads: int):
+    """Times the float64 CPU restatement of STEM.cpuScan on `n_positions` positions of the workload (transmissions
+    computed once, as runBatch shares them), `threads` positions at a time. Returns (steps/s, seconds, positions)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import simk_oracle as O
+    box, nums, pos = srtio3(8, 8, 20)
+    s = O.Structure(box, nums, pos)
+    p = O.Potential.from_structure(s, NX, NY, slice_thickness=SLICE, pi_choice="exact")
+    g = p.grid
+    ts = [O.transmission(v, ENERGY, g) for v in p.build()]
+    spec = O.ProbeSpec(ENERGY, SEMIANGLE)
+    dets = [O.DetectorSpec("annular", {"inner": a, "outer": b}) for _, a, b in DETECTORS]
+    positions = scan_positions()[:: max(1, (SCAN_N * SCAN_N) // n_positions)][:n_positions]
+
+    def one(q):
+        psi0 = O.build_probe(spec, g, positions[q])
+        ex = O.multislice(psi0, ts, p.thicknesses, ENERGY, g)[-1]
+        pat = O.diffraction_intensity(ex)
+        return [d.detect(pat, g, ENERGY) for d in dets]
+
+    one(0)  # warm-up
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(one, range(len(positions))))
+    dt = time.perf_counter() - t0
+    return len(positions) * len(p.thicknesses) / dt, dt, len(positions)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = min(8, os.cpu_count() or 1)
+    n_pos = args.cpu_positions
+    vals = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    for _ in range(args.steps):
+        v, dt, n = cpu_reference(n_pos, threads)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"metric": "probe.slice steps/s", "value": value, "unit": "probe.slice steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n * 20 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": {"workload": WORKLOAD, "form": "cpu float64"},
+            "cpu_baseline": {"value": value, "unit": "probe.slice steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{n} of 4096 positions x 20 slices per step, float64 NumPy restatement of "
+                                       f"STEM.cpuScan, {threads} threads over positions"},
+            "e2e": {"value": value, "unit": "probe.slice steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fused", choices=["plain", "fused", "bf16x3"])
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--cpu-positions", type=int, default=32)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import ctypes as C
+
+    import simulatokit_b200 as sk
+    from simulatokit_b200 import _lib as L
+
+    engine = sk.Engine.require(local)
+    stream = torch.cuda.current_stream()
+    engine.set_stream(stream.cuda_stream)
+    opts = sk.ExecutionOptions(form=args.form, batch=args.batch)
+    engine.apply(opts)
+
+    box, nums, pos = srtio3(8, 8, 20)
+    structure = sk.AtomicStructure(box, nums, pos)
+    pot = sk.Potential(structure, NX, NY, slice_thickness=SLICE)
+    assert pot.slice_count == 20
+    beam = sk.ElectronBeam(ENERGY)
+    probe = sk.Probe(beam, pot.grid, sk.Aperture(SEMIANGLE))
+    dets = [sk.AnnularDetector(a, b) for _, a, b in DETECTORS]
+    positions = scan_positions()
+    n_pos = len(positions)
+    steps_per_scan = n_pos * pot.slice_count
+
+    # device-resident inputs and outputs
+    h = pot.handle(engine)
+    pos_dev = torch.tensor(positions, dtype=torch.float64, device="cuda")
+    outs = [torch.zeros(n_pos, dtype=torch.float64, device="cuda") for _ in dets]
+    harr = (C.c_void_p * 1)(h.handle)
+    darr = (L.Detector_t * len(dets))(*[d.c() for d in dets])
+    oarr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+    pc = probe.c()
+
+    def scan_once():
+        L.check(engine.lib.simk_scan_device(engine.handle, C.byref(pc), 1, harr, n_pos, C.c_void_p(pos_dev.data_ptr()),
+                                            len(dets), darr, oarr))
+
+    for _ in range(max(3, args.warmup)):
+        scan_once()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    engine.set_timing(True)
+    engine.kernel_time("line_fft", reset=True)
+    engine.launch_count(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            scan_once()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = engine.launch_count()
+    names = ["fused_rows", "fused_cols", "line_fft", "pointwise", "detect"]
+    ktimes = {n: engine.kernel_time(n) for n in names}
+    engine.set_timing(False)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * steps_per_scan * args.steps / (ms_max / 1e3)
+
+    # dominant kernel: the largest total time
+    dom = max(ktimes, key=lambda n: ktimes[n][0])
+    dms, dn, dbytes = ktimes[dom]
+    peak, peak_kind = measured_peaks()
+    achieved = (dbytes / dn) / (dms / dn / 1e3) / 1e9 if dn else None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "traffic": traffic_from_profiles(f"{dom}@{args.form}"),
+                "algorithmic_bytes_per_launch": dbytes / dn if dn else None,
+                "avg_launch_ms": dms / dn if dn else None,
+                "kernel_share": {n: round(ktimes[n][0] / ms, 4) for n in names if ktimes[n][1]},
+                "step_bytes_rule": "32*N bytes per probe.slice step (two read+write passes of the complex64 wave)",
+                "step_roofline_frac": (value / world) * 32 * NX * NY / (peak * 1e9)}
+
+    # e2e: the public API from host arrays, potential built on the device each call
+    e2e_val = None
+    h2d = d2h = 0
+    if args.e2e_steps > 0:
+        scan = sk.GridScan((4 * A0, 4 * A0), (5 * A0, 5 * A0), SCAN_N, SCAN_N)
+        times = []
+        for it in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p2 = sk.Potential(structure, NX, NY, slice_thickness=SLICE)
+            res = sk.STEM.scan(probe, [p2], scan, dets, options=opts, engine=engine)
+            torch.cuda.synchronize()
+            if it > 0:
+                times.append(time.perf_counter() - t0)
+            del p2
+        e2e_val = world * steps_per_scan / statistics.median(times)
+        n_atoms = len(nums)
+        h2d = n_atoms * (4 + 24 + 4) + 20 * 8 + n_pos * 16
+        d2h = sum(n_pos * 8 for _ in dets)
+        engine.apply(opts)
+        engine.set_stream(stream.cuda_stream)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = min(8, os.cpu_count() or 1)
+        v, dt, n = cpu_reference(args.cpu_positions, threads)
+        cpu = {"value": v, "unit": "probe.slice steps/s", "cores": threads, "kind": "port",
+               "sample": f"{n} of 4096 positions x 20 slices ({dt:.1f} s), float64 NumPy restatement of STEM.cpuScan, "
+                         f"{threads} threads over positions"}
+
+    if rank == 0:
+        line = {"metric": "probe.slice steps/s", "value": value, "unit": "probe.slice steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "form": args.form, "positions": n_pos, "slices": 20,
+                           "grid": [NX, NY], "replicas": world, "l2": "inputs larger than L2 (batch of waves up to "
+                                                                     "1 GiB per launch)"},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+                "e2e": {"value": e2e_val, "unit": "probe.slice steps/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h}}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

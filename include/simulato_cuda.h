@@ -1,0 +1,178 @@
+/*
+ * simulato_cuda.h -- the C ABI of libsimulato_cuda.so, the `.cuda` backend of SimulatoKit's multislice hot path.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an `int` status (SIMK_OK = 0);
+ * `simk_last_error()` gives the message of the calling thread's last failure. Host buffers are owned by the caller and
+ * are not retained. Device memory is owned by the context and by the potential handles. One context serialises its
+ * calls with a mutex (the analogue of MetalEngine's `runLock`, Sources/SimulatoMultislice/MetalEngine.swift:51).
+ *
+ * Complex arrays cross the boundary as split float64 real / imaginary arrays, row-major [ix * ny + iy], the layout of
+ * SimulatoKit's `ComplexField` (Sources/SimulatoCore/Fields.swift:8-49), so a Swift caller passes `field.real` and
+ * `field.imaginary` directly. Inside, waves are interleaved complex64 [batch][ix][iy] in HBM.
+ *
+ * Each function names the reference interface it replaces. The Swift-side binding is shown in INTEGRATION.md.
+ */
+#ifndef SIMULATO_CUDA_H
+#define SIMULATO_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (mapped by the Swift side onto SimulatoError, Sources/SimulatoCore/SimulatoError.swift:7-57) ---- */
+#define SIMK_OK 0
+#define SIMK_ERR_INVALID 1       /* a refused argument: SimulatoError.invalid* / unsupported* */
+#define SIMK_ERR_CUDA 2          /* a CUDA failure: the .metalFailure(String) analogue */
+#define SIMK_ERR_UNAVAILABLE 3   /* no usable sm_100 device: the .metalUnavailable analogue */
+#define SIMK_ERR_MEMORY 4        /* device memory refused */
+#define SIMK_ERR_TIMEOUT 5       /* a bounded device wait ran out */
+
+/* ---- execution forms (the metric's A/B pair) ---- */
+#define SIMK_FORM_PLAIN 0   /* one operation per launch, FP32 Stockham FFT in shared memory */
+#define SIMK_FORM_FUSED 1   /* batched: transmission/propagator fused into register-resident FFT passes, FP32 */
+#define SIMK_FORM_BF16X3 2  /* FUSED with the radix DFT stages on tensor cores, 3-term split BF16, FP32 accumulate */
+
+/* ---- context options (the ExecutionOptions analogue, Sources/SimulatoMultislice/ExecutionOptions.swift:21-49) ---- */
+#define SIMK_OPT_FORM 0         /* one of SIMK_FORM_* (default SIMK_FORM_FUSED) */
+#define SIMK_OPT_BATCH 1        /* waves per batch, 0 = from SIMK_OPT_BATCH_BYTES (default 0) */
+#define SIMK_OPT_BATCH_BYTES 2  /* device bytes of waves one batch may hold (default 1 GiB) */
+#define SIMK_OPT_GRAPHS 3       /* capture the slice loop of a batch in a CUDA graph (default 1) */
+#define SIMK_OPT_TIMING 4       /* record CUDA events around every hot-path launch (default 0) */
+
+/* ---- Lobato pi choice (LobatoParameterization.PiConstant, LobatoParameterization.swift:15-24) ---- */
+#define SIMK_PI_EXACT 0
+#define SIMK_PI_ABTEM_FLOAT32 1
+
+/* ---- detector kinds (Sources/SimulatoDetector/Detectors.swift:91-263) ---- */
+#define SIMK_DET_ANNULAR 0
+#define SIMK_DET_PIXELATED 1
+#define SIMK_DET_COM 2
+#define SIMK_DET_SEGMENTED 3
+#define SIMK_MAXANGLE_CUTOFF 0   /* PixelatedDetector.MaxAngle */
+#define SIMK_MAXANGLE_VALID 1
+#define SIMK_MAXANGLE_FULL 2
+#define SIMK_UNITS_MRAD 0        /* CenterOfMassDetector.Units */
+#define SIMK_UNITS_INV_ANGSTROM 1
+
+typedef struct simk_context simk_context;
+typedef struct simk_potential simk_potential;
+
+/* Grid (Sources/SimulatoCore/Grid.swift:8-91): nx x ny points over extent_x x extent_y [A]. */
+typedef struct {
+    int32_t nx, ny;
+    double extent_x, extent_y;
+} simk_grid;
+
+/* Probe (Sources/SimulatoProbe/Probe.swift:51-70) with its Aberrations (Aberrations.swift:8-15), in the order
+ * C10 C12 phi12 C21 phi21 C23 phi23 C30 C32 phi32 C34 phi34 C41 phi41 C43 phi43 C45 phi45 C50 C52 phi52 C54 phi54
+ * C56 phi56 [A, rad]. semiangle_mrad = INFINITY for no aperture. */
+typedef struct {
+    double energy;
+    double semiangle_mrad;
+    int32_t soft;
+    int32_t reserved;
+    double aberrations[25];
+    double tilt_x, tilt_y;  /* [mrad] */
+} simk_probe;
+
+/* One detector (Detectors.swift:91-263). annular: inner, outer (has_outer = 0: the default outer angle);
+ * pixelated: max_angle; com: max_angle, units; segmented: nr, nphi, inner, outer, rotation [rad]. */
+typedef struct {
+    int32_t kind;
+    int32_t max_angle;
+    int32_t units;
+    int32_t has_outer;
+    int32_t nr, nphi;
+    double inner, outer, rotation;
+} simk_detector;
+
+/* ---- availability, context (Multislice.metalIsAvailable, MetalMultislice.swift:20; MetalEngine.require :72-77) --- */
+int simk_cuda_available(int32_t* device_count);
+const char* simk_last_error(void);
+int simk_context_create(int32_t device, simk_context** out);
+int simk_context_destroy(simk_context* ctx);
+/* Runs every later call of this context on `stream` (a cudaStream_t; NULL = the context's own stream). */
+int simk_context_set_stream(simk_context* ctx, void* stream);
+int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value);
+int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value);
+int simk_context_synchronize(simk_context* ctx);
+/* Kernels this context launched since the last reset (the bench's launch count). */
+int simk_context_launch_count(simk_context* ctx, int64_t* count, int32_t reset);
+/* With SIMK_OPT_TIMING on: the summed CUDA-event time [ms], launch count and algorithmic bytes of the hot-path kernel
+ * `name` ("line_fft", "pointwise", "detect", "fused_rows", "fused_cols") since the last reset. Synchronises. */
+int simk_context_kernel_time(simk_context* ctx, const char* name, double* total_ms, int64_t* launches,
+                             double* algorithmic_bytes, int32_t reset);
+
+/* ---- potentials ---------------------------------------------------------------------------------------------------
+ * From atoms: replaces MetalMultislice.prepare(Potential) (MetalEngine.swift:277-308) and Potential.build
+ * (Potential.swift:83-91, ProjectedPotential.swift:109-202). `xyz` are the wrapped positions (n_atoms x 3) and
+ * `slice_of_atom` the slice of each (Potential.init, Potential.swift:49-63); V is built on the device in float64
+ * (bilinear deltas, FFT, x f(k^2)/S(k), IFFT, summed over elements in increasing Z). */
+int simk_potential_from_atoms(simk_context* ctx, const simk_grid* grid, int32_t n_slices, const double* thickness,
+                              int32_t pi_choice, int32_t n_atoms, const int32_t* atomic_numbers, const double* xyz,
+                              const int32_t* slice_of_atom, simk_potential** out);
+/* From values: replaces MetalMultislice.prepare(ProjectedPotential) (MetalEngine.swift:310-321); values are
+ * n_slices x nx x ny float64 V [V A]. */
+int simk_potential_from_values(simk_context* ctx, const simk_grid* grid, int32_t n_slices, const double* thickness,
+                               const double* values, simk_potential** out);
+int simk_potential_destroy(simk_potential* potential);
+int simk_potential_slice_count(const simk_potential* potential, int32_t* n_slices);
+/* V of every slice as the device built it (n_slices x nx x ny): the gpuPotentialSlices test hook
+ * (MetalMultislice.swift:107-110). */
+int simk_potential_read_slices(simk_context* ctx, simk_potential* potential, double* values);
+/* The bandlimited transmission t of one slice for a beam energy (Multislice.transmissionFunctions,
+ * Multislice.swift:83-103), as stored on the device (complex64 widened). */
+int simk_potential_read_transmission(simk_context* ctx, simk_potential* potential, double energy, int32_t slice,
+                                     double* re, double* im);
+
+/* ---- multislice -----------------------------------------------------------------------------------------------------
+ * Multislice.run (Multislice.swift:52-80 -> MetalMultislice.run, MetalEngine.swift:458-474): one incident wave through
+ * the potential; returns the waves after the slices in `planes` (ascending, >= 0; the caller adds the incident for -1),
+ * n_planes x nx x ny. `normalization_values` = 1 for a plane-wave-normalised wave (ignored here; kept for symmetry). */
+int simk_run(simk_context* ctx, simk_potential* potential, double energy, double tilt_x, double tilt_y,
+             const double* in_re, const double* in_im, int32_t n_planes, const int32_t* planes,
+             double* out_re, double* out_im);
+/* Multislice.runBatch (MetalMultislice.swift:52-83 -> MetalEngine.swift:476-501): `count` incident waves, the exit
+ * wave of each after the last slice. */
+int simk_run_batch(simk_context* ctx, simk_potential* potential, double energy, double tilt_x, double tilt_y,
+                   int32_t count, const double* in_re, const double* in_im, double* out_re, double* out_im);
+
+/* ---- probes -------------------------------------------------------------------------------------------------------
+ * Probe.centredSpectrum (Probe.swift:113-136) computed on the device in float64. */
+int simk_probe_spectrum(simk_context* ctx, const simk_grid* grid, const simk_probe* probe, double* re, double* im);
+/* The probes IFFT(Psi0 . r_x (x) r_y) at `count` positions (x, y) [A]: the gpuProbes test hook
+ * (MetalMultislice.swift:113-117); equals Probe.build(at:) (Probe.swift:72-109). */
+int simk_build_probes(simk_context* ctx, const simk_grid* grid, const simk_probe* probe, int32_t count,
+                      const double* positions_xy, double* out_re, double* out_im);
+
+/* ---- detectors and the STEM scan -----------------------------------------------------------------------------------
+ * The value shape of one position for a detector (Detector.shape(for:beam:), Detectors.swift:84-88): writes ndim
+ * (0, 1 or 2) and the sizes. */
+int simk_detector_shape(const simk_grid* grid, double energy, const simk_detector* detector, int32_t* ndim,
+                        int32_t* shape);
+/* STEM.scan (STEM.swift:49-80, 95-150; Metal arm MetalEngine.swift:583-677): the probe at every position through every
+ * potential (one per frozen-phonon configuration), every detector on |FFT2(exit)|^2 on the device, the mean over
+ * potentials. outputs[d] holds n_positions x (the detector's value count) float64, row-major. */
+int simk_scan(simk_context* ctx, const simk_probe* probe, int32_t n_potentials, simk_potential* const* potentials,
+              int32_t n_positions, const double* positions_xy, int32_t n_detectors, const simk_detector* detectors,
+              double* const* outputs);
+/* The same with every buffer already on the device: positions_xy is a device pointer (n_positions x 2 float64) and
+ * outputs[d] are device pointers; nothing is copied to or from the host and the call does not synchronise. */
+int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_potentials,
+                     simk_potential* const* potentials, int32_t n_positions, const double* positions_xy_device,
+                     int32_t n_detectors, const simk_detector* detectors, double* const* outputs_device);
+
+/* ---- the transform itself (FFT2D, Sources/SimulatoCore/FFT2D.swift:169-265) ----------------------------------------
+ * `count` nx x ny fields, forward (unnormalised, e^{-2 pi i}) or inverse (x 1/(nx ny)), in float32 (precision 32) or
+ * float64 (precision 64) on the device. A test hook: the hot path calls the transforms internally. */
+int simk_fft2(simk_context* ctx, int32_t nx, int32_t ny, int32_t count, int32_t inverse, int32_t precision,
+              const double* in_re, const double* in_im, double* out_re, double* out_im);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIMULATO_CUDA_H */

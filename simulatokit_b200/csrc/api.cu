@@ -1,0 +1,477 @@
+// api.cu -- the extern "C" entry points of libsimulato_cuda.so (declared in include/simulato_cuda.h).
+// Every call catches C++ exceptions and turns them into a status code plus a thread-local message.
+#include <cstring>
+#include <string>
+
+#include "context.cuh"
+#include "engine.cuh"
+
+using namespace simk;
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return SIMK_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host memory exhausted";
+        return SIMK_ERR_MEMORY;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return SIMK_ERR_CUDA;
+    }
+}
+
+GridGeom geom_of(const simk_grid* g) {
+    SIMK_REQUIRE(g != nullptr, "grid is null");
+    SIMK_REQUIRE(g->nx >= 2 && g->ny >= 2, "grid lengths must be at least 2 (Grid.isSupportedLength)");
+    SIMK_REQUIRE(std::isfinite(g->extent_x) && std::isfinite(g->extent_y) && g->extent_x > 0 && g->extent_y > 0,
+                 "the extent must be finite and positive");
+    SIMK_REQUIRE((long long)g->nx * g->ny <= (1LL << 28), "grid too large");
+    GridGeom r;
+    r.nx = g->nx;
+    r.ny = g->ny;
+    r.ex = g->extent_x;
+    r.ey = g->extent_y;
+    return r;
+}
+
+void activate(Context& c) { SIMK_CUDA(cudaSetDevice(c.device)); }
+
+std::vector<double> checked_thickness(int32_t n_slices, const double* thickness) {
+    SIMK_REQUIRE(n_slices >= 1 && thickness != nullptr, "a potential needs at least one slice");
+    std::vector<double> dz(thickness, thickness + n_slices);
+    for (double d : dz) SIMK_REQUIRE(std::isfinite(d) && d > 0, "slice thicknesses must be finite and positive");
+    return dz;
+}
+}  // namespace
+
+extern "C" {
+
+int simk_cuda_available(int32_t* device_count) {
+    return guarded([&] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+        int usable = 0;
+        for (int d = 0; d < n; ++d) {
+            cudaDeviceProp p;
+            if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major >= 10) ++usable;
+        }
+        if (device_count) *device_count = usable;
+        if (usable == 0) throw Error(SIMK_ERR_UNAVAILABLE, "no CUDA device of compute capability 10.x or later");
+    });
+}
+
+const char* simk_last_error(void) { return g_last_error.c_str(); }
+
+int simk_context_create(int32_t device, simk_context** out) {
+    return guarded([&] {
+        SIMK_REQUIRE(out != nullptr, "out is null");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw Error(SIMK_ERR_UNAVAILABLE, "no CUDA device");
+        SIMK_REQUIRE(device >= 0 && device < n, "device index out of range");
+        cudaDeviceProp p;
+        SIMK_CUDA(cudaGetDeviceProperties(&p, device));
+        if (p.major < 10) throw Error(SIMK_ERR_UNAVAILABLE, "the library is built for sm_100a (B200)");
+        auto* c = new simk_context();
+        c->impl.device = device;
+        try {
+            SIMK_CUDA(cudaSetDevice(device));
+            SIMK_CUDA(cudaStreamCreateWithFlags(&c->impl.own_stream, cudaStreamNonBlocking));
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        c->impl.stream = c->impl.own_stream;
+        *out = c;
+    });
+}
+
+int simk_context_destroy(simk_context* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->impl.device);
+        cudaStreamSynchronize(ctx->impl.stream);
+        cudaStream_t s = ctx->impl.own_stream;
+        delete ctx;
+        if (s) cudaStreamDestroy(s);
+    });
+}
+
+int simk_context_set_stream(simk_context* ctx, void* stream) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx, "context is null");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        ctx->impl.stream = stream ? static_cast<cudaStream_t>(stream) : ctx->impl.own_stream;
+    });
+}
+
+int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx, "context is null");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        Context& c = ctx->impl;
+        switch (option) {
+            case SIMK_OPT_FORM:
+                SIMK_REQUIRE(value == SIMK_FORM_PLAIN || value == SIMK_FORM_FUSED || value == SIMK_FORM_BF16X3,
+                             "unknown form");
+                c.form = (int)value;
+                break;
+            case SIMK_OPT_BATCH: SIMK_REQUIRE(value >= 0, "batch must be >= 0"); c.batch = value; break;
+            case SIMK_OPT_BATCH_BYTES: c.batch_bytes = std::max<int64_t>(1, value); break;
+            case SIMK_OPT_GRAPHS: c.graphs = value ? 1 : 0; break;
+            case SIMK_OPT_TIMING: c.timing = value ? 1 : 0; break;
+            default: throw Error(SIMK_ERR_INVALID, "unknown option");
+        }
+    });
+}
+
+int simk_context_kernel_time(simk_context* ctx, const char* name, double* total_ms, int64_t* launches,
+                             double* algorithmic_bytes, int32_t reset) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && name && total_ms && launches && algorithmic_bytes, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+        ctx->impl.times.collect();
+        auto it = ctx->impl.times.done.find(name);
+        if (it == ctx->impl.times.done.end()) {
+            *total_ms = 0;
+            *launches = 0;
+            *algorithmic_bytes = 0;
+        } else {
+            *total_ms = std::get<0>(it->second);
+            *launches = std::get<1>(it->second);
+            *algorithmic_bytes = std::get<2>(it->second);
+        }
+        if (reset) ctx->impl.times.done.clear();
+    });
+}
+
+int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && value, "null argument");
+        Context& c = ctx->impl;
+        switch (option) {
+            case SIMK_OPT_FORM: *value = c.form; break;
+            case SIMK_OPT_BATCH: *value = c.batch; break;
+            case SIMK_OPT_BATCH_BYTES: *value = c.batch_bytes; break;
+            case SIMK_OPT_GRAPHS: *value = c.graphs; break;
+            case SIMK_OPT_TIMING: *value = c.timing; break;
+            default: throw Error(SIMK_ERR_INVALID, "unknown option");
+        }
+    });
+}
+
+int simk_context_synchronize(simk_context* ctx) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx, "context is null");
+        activate(ctx->impl);
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+    });
+}
+
+int simk_context_launch_count(simk_context* ctx, int64_t* count, int32_t reset) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && count, "null argument");
+        *count = ctx->impl.launches;
+        if (reset) ctx->impl.launches = 0;
+    });
+}
+
+// ---- potentials ------------------------------------------------------------------------------------------------------
+int simk_potential_from_atoms(simk_context* ctx, const simk_grid* grid, int32_t n_slices, const double* thickness,
+                              int32_t pi_choice, int32_t n_atoms, const int32_t* atomic_numbers, const double* xyz,
+                              const int32_t* slice_of_atom, simk_potential** out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && out, "null argument");
+        SIMK_REQUIRE(n_atoms >= 0, "negative atom count");
+        SIMK_REQUIRE(n_atoms == 0 || (atomic_numbers && xyz && slice_of_atom), "null atom arrays");
+        SIMK_REQUIRE(pi_choice == SIMK_PI_EXACT || pi_choice == SIMK_PI_ABTEM_FLOAT32, "unknown pi choice");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        auto p = std::make_unique<simk_potential>();
+        p->impl.ctx = &ctx->impl;
+        p->impl.g = geom_of(grid);
+        p->impl.dz = checked_thickness(n_slices, thickness);
+        build_potential_from_atoms(ctx->impl, p->impl, pi_choice, n_atoms, atomic_numbers, xyz, slice_of_atom);
+        *out = p.release();
+    });
+}
+
+int simk_potential_from_values(simk_context* ctx, const simk_grid* grid, int32_t n_slices, const double* thickness,
+                               const double* values, simk_potential** out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && out && values, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        auto p = std::make_unique<simk_potential>();
+        p->impl.ctx = &ctx->impl;
+        p->impl.g = geom_of(grid);
+        p->impl.dz = checked_thickness(n_slices, thickness);
+        const size_t bytes = (size_t)n_slices * p->impl.g.count() * sizeof(double);
+        p->impl.V.alloc(bytes);
+        SIMK_CUDA(cudaMemcpy(p->impl.V.ptr, values, bytes, cudaMemcpyHostToDevice));
+        *out = p.release();
+    });
+}
+
+int simk_potential_destroy(simk_potential* potential) {
+    return guarded([&] {
+        if (!potential) return;
+        if (potential->impl.ctx) cudaSetDevice(potential->impl.ctx->device);
+        delete potential;
+    });
+}
+
+int simk_potential_slice_count(const simk_potential* potential, int32_t* n_slices) {
+    return guarded([&] {
+        SIMK_REQUIRE(potential && n_slices, "null argument");
+        *n_slices = potential->impl.n_slices();
+    });
+}
+
+int simk_potential_read_slices(simk_context* ctx, simk_potential* potential, double* values) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && potential && values, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+        SIMK_CUDA(cudaMemcpy(values, potential->impl.V.ptr,
+                             (size_t)potential->impl.n_slices() * potential->impl.g.count() * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    });
+}
+
+int simk_potential_read_transmission(simk_context* ctx, simk_potential* potential, double energy, int32_t slice,
+                                     double* re, double* im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && potential && re && im, "null argument");
+        SIMK_REQUIRE(std::isfinite(energy) && energy > 0, "the energy must be finite and positive");
+        SIMK_REQUIRE(slice >= 0 && slice < potential->impl.n_slices(), "slice out of range");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        prepare_transmissions(ctx->impl, potential->impl, energy);
+        const long long N = potential->impl.g.count();
+        std::vector<float2> h(N);
+        SIMK_CUDA(cudaMemcpy(h.data(), potential->impl.t.as<float2>() + slice * N, N * sizeof(float2),
+                             cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < N; ++i) {
+            re[i] = h[i].x;
+            im[i] = h[i].y;
+        }
+    });
+}
+
+// ---- multislice ------------------------------------------------------------------------------------------------------
+int simk_run(simk_context* ctx, simk_potential* potential, double energy, double tilt_x, double tilt_y,
+             const double* in_re, const double* in_im, int32_t n_planes, const int32_t* planes, double* out_re,
+             double* out_im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && potential && in_re && in_im && out_re && out_im && planes, "null argument");
+        SIMK_REQUIRE(std::isfinite(energy) && energy > 0, "the energy must be finite and positive");
+        SIMK_REQUIRE(std::isfinite(tilt_x) && std::isfinite(tilt_y), "the tilt must be finite");
+        const int S = potential->impl.n_slices();
+        SIMK_REQUIRE(n_planes >= 1, "at least one exit plane");
+        std::vector<int> pl(planes, planes + n_planes);
+        for (int q = 0; q < n_planes; ++q) {
+            SIMK_REQUIRE(pl[q] >= 0 && pl[q] < S, "exit planes must lie within 0 ..< slice count");
+            SIMK_REQUIRE(q == 0 || pl[q] > pl[q - 1], "exit planes must be ascending and distinct");
+        }
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        run_waves(ctx->impl, potential->impl, energy, tilt_x, tilt_y, 1, in_re, in_im, pl, out_re, out_im);
+    });
+}
+
+int simk_run_batch(simk_context* ctx, simk_potential* potential, double energy, double tilt_x, double tilt_y,
+                   int32_t count, const double* in_re, const double* in_im, double* out_re, double* out_im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && potential, "null argument");
+        SIMK_REQUIRE(count >= 0, "negative count");
+        if (count == 0) return;
+        SIMK_REQUIRE(in_re && in_im && out_re && out_im, "null argument");
+        SIMK_REQUIRE(std::isfinite(energy) && energy > 0, "the energy must be finite and positive");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        std::vector<int> pl{potential->impl.n_slices() - 1};
+        run_waves(ctx->impl, potential->impl, energy, tilt_x, tilt_y, count, in_re, in_im, pl, out_re, out_im);
+    });
+}
+
+// ---- probes ------------------------------------------------------------------------------------------------------------
+int simk_probe_spectrum(simk_context* ctx, const simk_grid* grid, const simk_probe* probe, double* re, double* im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && probe && re && im, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        GridGeom g = geom_of(grid);
+        DeviceBuffer f32, f64;
+        probe_spectrum_device(ctx->impl, g, *probe, f32, &f64);
+        std::vector<double2> h(g.count());
+        SIMK_CUDA(cudaMemcpy(h.data(), f64.ptr, g.count() * sizeof(double2), cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < g.count(); ++i) {
+            re[i] = h[i].x;
+            im[i] = h[i].y;
+        }
+    });
+}
+
+int simk_build_probes(simk_context* ctx, const simk_grid* grid, const simk_probe* probe, int32_t count,
+                      const double* positions_xy, double* out_re, double* out_im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && probe, "null argument");
+        SIMK_REQUIRE(count >= 0, "negative count");
+        if (count == 0) return;
+        SIMK_REQUIRE(positions_xy && out_re && out_im, "null argument");
+        for (int i = 0; i < 2 * count; ++i)
+            SIMK_REQUIRE(std::isfinite(positions_xy[i]), "invalid position " + std::to_string(i / 2));
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        GridGeom g = geom_of(grid);
+        const long long N = g.count();
+        DeviceBuffer spectrum, pos(2 * count * sizeof(double)), rx(count * g.nx * sizeof(float2)),
+            ry(count * g.ny * sizeof(float2)), psi(count * N * sizeof(float2));
+        probe_spectrum_device(c, g, *probe, spectrum, nullptr);
+        SIMK_CUDA(cudaMemcpyAsync(pos.ptr, positions_xy, 2 * count * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        launch_ramps(c, g, pos.as<double>(), 0, count, rx.as<float2>(), ry.as<float2>());
+        launch_probes(c, g, spectrum.as<float2>(), rx.as<float2>(), ry.as<float2>(), count, psi.as<float2>(), 1.0f);
+        fft2(c.plan(g.ny, 32), c.plan(g.nx, 32), psi.ptr, g.nx, g.ny, count, +1, 1.0 / (double)N, c.stream,
+             &c.launches);
+        std::vector<float2> h(count * N);
+        SIMK_CUDA(cudaMemcpyAsync(h.data(), psi.ptr, count * N * sizeof(float2), cudaMemcpyDeviceToHost, c.stream));
+        SIMK_CUDA(cudaStreamSynchronize(c.stream));
+        for (long long i = 0; i < count * N; ++i) {
+            out_re[i] = h[i].x;
+            out_im[i] = h[i].y;
+        }
+    });
+}
+
+// ---- detectors and scans ---------------------------------------------------------------------------------------------
+int simk_detector_shape(const simk_grid* grid, double energy, const simk_detector* detector, int32_t* ndim,
+                        int32_t* shape) {
+    return guarded([&] {
+        SIMK_REQUIRE(detector && ndim && shape, "null argument");
+        GridGeom g = geom_of(grid);
+        int nd = 0, sh[2] = {0, 0};
+        detector_shape(g, energy, *detector, &nd, sh);
+        *ndim = nd;
+        shape[0] = sh[0];
+        shape[1] = sh[1];
+    });
+}
+
+namespace {
+std::vector<PotentialImpl*> potentials_of(int32_t n, simk_potential* const* p) {
+    SIMK_REQUIRE(n >= 1 && p, "no potential");
+    std::vector<PotentialImpl*> v;
+    for (int i = 0; i < n; ++i) {
+        SIMK_REQUIRE(p[i] != nullptr, "null potential");
+        v.push_back(&p[i]->impl);
+    }
+    return v;
+}
+}  // namespace
+
+int simk_scan(simk_context* ctx, const simk_probe* probe, int32_t n_potentials, simk_potential* const* potentials,
+              int32_t n_positions, const double* positions_xy, int32_t n_detectors, const simk_detector* detectors,
+              double* const* outputs) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && probe, "null argument");
+        SIMK_REQUIRE(n_positions >= 1 && positions_xy, "no scan position");
+        SIMK_REQUIRE(n_detectors >= 0 && n_detectors <= 16 && (n_detectors == 0 || (detectors && outputs)),
+                     "0 to 16 detectors");
+        for (int i = 0; i < 2 * n_positions; ++i)
+            SIMK_REQUIRE(std::isfinite(positions_xy[i]), "invalid position " + std::to_string(i / 2));
+        auto pots = potentials_of(n_potentials, potentials);
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        const GridGeom& g = pots[0]->g;
+        std::vector<long long> counts(n_detectors);
+        for (int d = 0; d < n_detectors; ++d) {
+            int nd, sh[2] = {1, 1};
+            detector_shape(g, probe->energy, detectors[d], &nd, sh);
+            counts[d] = nd == 0 ? 1 : nd == 1 ? sh[0] : (long long)sh[0] * sh[1];
+        }
+        c.positions.ensure(2 * n_positions * sizeof(double));
+        SIMK_CUDA(cudaMemcpyAsync(c.positions.ptr, positions_xy, 2 * n_positions * sizeof(double),
+                                  cudaMemcpyHostToDevice, c.stream));
+        if ((int)c.outputs.size() < n_detectors) c.outputs.resize(n_detectors);
+        std::vector<double*> dev_out(n_detectors);
+        for (int d = 0; d < n_detectors; ++d) {
+            c.outputs[d].ensure(n_positions * counts[d] * sizeof(double));
+            dev_out[d] = c.outputs[d].as<double>();
+        }
+        scan_device(c, *probe, pots, n_positions, c.positions.as<double>(), n_detectors, detectors, dev_out.data());
+        for (int d = 0; d < n_detectors; ++d)
+            SIMK_CUDA(cudaMemcpyAsync(outputs[d], dev_out[d], n_positions * counts[d] * sizeof(double),
+                                      cudaMemcpyDeviceToHost, c.stream));
+        SIMK_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_potentials,
+                     simk_potential* const* potentials, int32_t n_positions, const double* positions_xy_device,
+                     int32_t n_detectors, const simk_detector* detectors, double* const* outputs_device) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && probe, "null argument");
+        SIMK_REQUIRE(n_positions >= 1 && positions_xy_device, "no scan position");
+        SIMK_REQUIRE(n_detectors >= 0 && n_detectors <= 16 && (n_detectors == 0 || (detectors && outputs_device)),
+                     "0 to 16 detectors");
+        auto pots = potentials_of(n_potentials, potentials);
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        scan_device(ctx->impl, *probe, pots, n_positions, positions_xy_device, n_detectors, detectors, outputs_device);
+    });
+}
+
+int simk_fft2(simk_context* ctx, int32_t nx, int32_t ny, int32_t count, int32_t inverse, int32_t precision,
+              const double* in_re, const double* in_im, double* out_re, double* out_im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && in_re && in_im && out_re && out_im, "null argument");
+        SIMK_REQUIRE(nx >= 1 && ny >= 1 && count >= 1, "sizes must be positive");
+        SIMK_REQUIRE(precision == 32 || precision == 64, "precision is 32 or 64");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        const long long N = (long long)nx * ny, total = N * count;
+        const double scale = inverse ? 1.0 / (double)N : 1.0;
+        if (precision == 64) {
+            std::vector<double2> h(total);
+            for (long long i = 0; i < total; ++i) h[i] = make_double2(in_re[i], in_im[i]);
+            DeviceBuffer d(total * sizeof(double2));
+            SIMK_CUDA(cudaMemcpy(d.ptr, h.data(), total * sizeof(double2), cudaMemcpyHostToDevice));
+            fft2(c.plan(ny, 64), c.plan(nx, 64), d.ptr, nx, ny, count, inverse ? +1 : -1, scale, c.stream, &c.launches);
+            SIMK_CUDA(cudaStreamSynchronize(c.stream));
+            SIMK_CUDA(cudaMemcpy(h.data(), d.ptr, total * sizeof(double2), cudaMemcpyDeviceToHost));
+            for (long long i = 0; i < total; ++i) {
+                out_re[i] = h[i].x;
+                out_im[i] = h[i].y;
+            }
+        } else {
+            std::vector<float2> h(total);
+            for (long long i = 0; i < total; ++i) h[i] = make_float2((float)in_re[i], (float)in_im[i]);
+            DeviceBuffer d(total * sizeof(float2));
+            SIMK_CUDA(cudaMemcpy(d.ptr, h.data(), total * sizeof(float2), cudaMemcpyHostToDevice));
+            fft2(c.plan(ny, 32), c.plan(nx, 32), d.ptr, nx, ny, count, inverse ? +1 : -1, scale, c.stream, &c.launches);
+            SIMK_CUDA(cudaStreamSynchronize(c.stream));
+            SIMK_CUDA(cudaMemcpy(h.data(), d.ptr, total * sizeof(float2), cudaMemcpyDeviceToHost));
+            for (long long i = 0; i < total; ++i) {
+                out_re[i] = h[i].x;
+                out_im[i] = h[i].y;
+            }
+        }
+    });
+}
+
+}  // extern "C"

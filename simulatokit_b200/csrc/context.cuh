@@ -1,0 +1,171 @@
+// context.cuh -- the library's context (stream, options, plan and table caches) and its potential handle.
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+
+struct simk_context;
+struct simk_potential;
+
+namespace simk {
+
+// Device view of a grid for kernels.
+struct GridDev {
+    int nx, ny;
+    double dx, dy;
+};
+inline GridDev grid_dev(const GridGeom& g) { return GridDev{g.nx, g.ny, g.dx(), g.dy()}; }
+
+// One reduction channel set of a detector (annular: 1, COM: 2, segmented: nr * nphi): the pixels of every channel as a
+// CSR list (pixel index, weight), channels of all detectors concatenated.
+struct DetectorPlan {
+    int n_channels = 0;
+    std::vector<int> det_first_channel;    // per detector: its first reduction channel (-1: pixelated)
+    std::vector<int> det_count;            // per detector: values per position
+    std::vector<int> det_pixelated_offset; // per detector: offset of its crop map (pixelated), -1 otherwise
+    DeviceBuffer chan_ptr;   // int32 [n_channels + 1]
+    DeviceBuffer chan_pix;   // int32 [total]
+    DeviceBuffer chan_w;     // float [total]
+    DeviceBuffer crop_src;   // int32, concatenated crop maps of the pixelated detectors
+    long long total_entries = 0;
+    long long total_crop = 0;
+    std::vector<int> host_chan_ptr;
+};
+
+struct Propagator {
+    DeviceBuffer p;  // float2 [N]: exp(-i pi lambda dz k^2) A (x tilt phase)
+};
+
+struct Context;
+
+struct PotentialImpl {
+    Context* ctx = nullptr;
+    GridGeom g;
+    std::vector<double> dz;
+    DeviceBuffer V;          // double [S][N], as built
+    double t_energy = -1.0;  // energy the transmissions below were built for
+    DeviceBuffer t;          // float2 [S][N]
+    int n_slices() const { return (int)dz.size(); }
+};
+
+// Per-kernel CUDA-event timing (SIMK_OPT_TIMING): events recorded around each launch of a named kernel, with the
+// launch's algorithmic bytes, summed when queried.
+struct KernelTimes {
+    struct Rec {
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::map<std::string, std::vector<Rec>> pending;
+    std::map<std::string, std::tuple<double, long long, double>> done;  // ms, launches, bytes
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        SIMK_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    void collect() {
+        for (auto& kv : pending) {
+            auto& d = done[kv.first];
+            for (auto& r : kv.second) {
+                float ms = 0;
+                SIMK_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+                std::get<0>(d) += ms;
+                std::get<1>(d) += 1;
+                std::get<2>(d) += r.bytes;
+                pool.push_back(r.a);
+                pool.push_back(r.b);
+            }
+        }
+        pending.clear();
+    }
+    ~KernelTimes() {
+        for (auto& kv : pending)
+            for (auto& r : kv.second) {
+                cudaEventDestroy(r.a);
+                cudaEventDestroy(r.b);
+            }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+struct Context {
+    int device = 0;
+    int timing = 0;
+    KernelTimes times;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    int form = SIMK_FORM_FUSED;
+    long long batch = 0;
+    long long batch_bytes = 1LL << 30;
+    int graphs = 1;
+    int64_t launches = 0;
+    std::map<std::pair<int, int>, std::unique_ptr<LinePlan>> plans;
+    std::map<std::tuple<int, int, double, double, double, double, double, double>, std::unique_ptr<Propagator>> props;
+    // workspaces
+    DeviceBuffer work_a, work_b, work_c, rx, ry, positions, partial;
+    std::vector<DeviceBuffer> outputs;
+
+    const LinePlan& plan(int n, int precision) {
+        auto key = std::make_pair(n, precision);
+        auto it = plans.find(key);
+        if (it != plans.end()) return *it->second;
+        auto p = make_line_plan(n, precision);
+        auto& ref = *p;
+        plans[key] = std::move(p);
+        return ref;
+    }
+    const Propagator& propagator(const GridGeom& g, double energy, double dz, double tx, double ty);
+};
+
+// Records events around one launch of kernel `name` when the context's timing is on.
+struct KernelTimer {
+    Context& c;
+    const char* name;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    KernelTimer(Context& ctx, const char* n, double algorithmic_bytes) : c(ctx), name(n), bytes(algorithmic_bytes) {
+        if (c.timing) {
+            a = c.times.get();
+            SIMK_CUDA(cudaEventRecord(a, c.stream));
+        }
+    }
+    ~KernelTimer() {
+        if (a) {
+            cudaEvent_t b = c.times.get();
+            cudaEventRecord(b, c.stream);
+            c.times.pending[name].push_back({a, b, bytes});
+        }
+    }
+};
+
+// kernels and helpers of physics.cu
+void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice, int n_atoms, const int* Z,
+                                const double* xyz, const int* slice_of_atom);
+void prepare_transmissions(Context& ctx, PotentialImpl& pot, double energy);
+void probe_spectrum_device(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
+                           DeviceBuffer* out_f64);
+void launch_ramps(Context& ctx, const GridGeom& g, const double* positions_dev, long long first, int count,
+                  float2* rx, float2* ry);
+void launch_probes(Context& ctx, const GridGeom& g, const float2* spectrum, const float2* rx, const float2* ry,
+                   int count, float2* out, float scale);
+void launch_mul_broadcast(Context& ctx, float2* psi, const float2* factor, long long n, int count, float scale);
+std::unique_ptr<DetectorPlan> build_detector_plan(Context& ctx, const GridGeom& g, double energy,
+                                                  const simk_detector* dets, int n_dets);
+void detector_shape(const GridGeom& g, double energy, const simk_detector& d, int* ndim, int* shape);
+void launch_detect(Context& ctx, const DetectorPlan& plan, const GridGeom& g, const float2* phi, int count,
+                   long long first_position, double* const* outputs_dev, double weight, float intensity_scale);
+
+}  // namespace simk
+
+struct simk_context {
+    simk::Context impl;
+};
+struct simk_potential {
+    simk::PotentialImpl impl;
+};

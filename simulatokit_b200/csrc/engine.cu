@@ -1,0 +1,149 @@
+// engine.cu -- the multislice loop on the device: Multislice.run / runBatch and the STEM scan, in the plain form
+// (one operation per launch over a batch of waves) and the fused form (fused.cu).
+#include <algorithm>
+#include <cstring>
+
+#include "context.cuh"
+#include "engine.cuh"
+
+namespace simk {
+
+// fft2 with each line pass timed as "line_fft" (algorithmic bytes: one read and one write of every element).
+void fft2_timed(Context& ctx, const LinePlan& prow, const LinePlan& pcol, float2* data, int nx, int ny, long long count,
+                int dir, double scale) {
+    const long long N = (long long)nx * ny;
+    const double bytes = 16.0 * (double)N * (double)count;
+    {
+        KernelTimer t(ctx, "line_fft", bytes);
+        launch_line_fft(prow, data, count * nx, nx, ny, 1, N, dir, 1.0, ctx.stream, &ctx.launches);
+    }
+    {
+        KernelTimer t(ctx, "line_fft", bytes);
+        launch_line_fft(pcol, data, count * ny, ny, 1, ny, N, dir, scale, ctx.stream, &ctx.launches);
+    }
+}
+
+void mul_timed(Context& ctx, float2* psi, const float2* f, long long N, int count, float scale) {
+    KernelTimer t(ctx, "pointwise", 16.0 * (double)N * (double)count);
+    launch_mul_broadcast(ctx, psi, f, N, count, scale);
+}
+
+long long batch_size(const Context& ctx, const GridGeom& g, long long count) {
+    long long b = ctx.batch;
+    if (b <= 0) b = std::max<long long>(1, ctx.batch_bytes / (long long)(g.count() * sizeof(float2)));
+    return std::max<long long>(1, std::min(b, count));
+}
+
+// psi (count waves, float2, on the device) through every slice of the potential, plain form. After slice j,
+// on_slice(j) is called (stream-ordered) so the caller can copy planes out.
+void propagate_plain(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
+                     bool last_inverse, const std::function<void(int)>& on_slice) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    const LinePlan& prow = ctx.plan(g.ny, 32);
+    const LinePlan& pcol = ctx.plan(g.nx, 32);
+    const int S = pot.n_slices();
+    for (int j = 0; j < S; ++j) {
+        const Propagator& P = ctx.propagator(g, energy, pot.dz[j], tx, ty);
+        mul_timed(ctx, psi, pot.t.as<float2>() + (long long)j * N, N, count, 1.0f);
+        fft2_timed(ctx, prow, pcol, psi, g.nx, g.ny, count, -1, 1.0);
+        mul_timed(ctx, psi, P.p.as<float2>(), N, count, 1.0f / (float)N);
+        if (j < S - 1 || last_inverse) fft2_timed(ctx, prow, pcol, psi, g.nx, g.ny, count, +1, 1.0);
+        if (on_slice) on_slice(j);
+    }
+}
+
+void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, int count, const double* in_re,
+               const double* in_im, const std::vector<int>& planes, double* out_re, double* out_im) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    prepare_transmissions(ctx, pot, energy);
+    const long long B = batch_size(ctx, g, count);
+    ctx.work_a.ensure(B * N * sizeof(float2));
+    std::vector<float2> host(B * N);
+    const int np = (int)planes.size();
+    for (long long first = 0; first < count; first += B) {
+        const int b = (int)std::min<long long>(B, count - first);
+        for (long long i = 0; i < b * N; ++i)
+            host[i] = make_float2((float)in_re[first * N + i], (float)in_im[first * N + i]);
+        SIMK_CUDA(cudaMemcpyAsync(ctx.work_a.ptr, host.data(), b * N * sizeof(float2), cudaMemcpyHostToDevice,
+                                  ctx.stream));
+        float2* psi = ctx.work_a.as<float2>();
+        auto copy_out = [&](int j) {
+            for (int q = 0; q < np; ++q) {
+                if (planes[q] != j) continue;
+                SIMK_CUDA(cudaMemcpyAsync(host.data(), psi, b * N * sizeof(float2), cudaMemcpyDeviceToHost, ctx.stream));
+                SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+                // output layout: [wave][plane][N] for run (count = 1) and [wave][N] for run_batch (one plane)
+                for (int w = 0; w < b; ++w)
+                    for (long long i = 0; i < N; ++i) {
+                        const long long o = ((first + w) * np + q) * N + i;
+                        out_re[o] = host[w * N + i].x;
+                        out_im[o] = host[w * N + i].y;
+                    }
+            }
+        };
+        propagate_plain(ctx, pot, energy, tx, ty, psi, b, true, copy_out);
+    }
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+namespace {
+void scan_plain_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
+                      double* const* outputs_dev, double weight) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    const LinePlan& prow = ctx.plan(g.ny, 32);
+    const LinePlan& pcol = ctx.plan(g.nx, 32);
+    float2* psi = ctx.work_a.as<float2>();
+    launch_ramps(ctx, g, positions_dev, first, b, ctx.rx.as<float2>(), ctx.ry.as<float2>());
+    launch_probes(ctx, g, spectrum, ctx.rx.as<float2>(), ctx.ry.as<float2>(), b, psi, 1.0f);
+    fft2_timed(ctx, prow, pcol, psi, g.nx, g.ny, b, +1, 1.0 / (double)N);
+    propagate_plain(ctx, pot, probe.energy, probe.tilt_x, probe.tilt_y, psi, b, true, nullptr);
+    // the diffraction intensity |FFT2(exit)|^2 (DiffractionIntensity, Detectors.swift:28-36)
+    fft2_timed(ctx, prow, pcol, psi, g.nx, g.ny, b, -1, 1.0);
+    {
+        KernelTimer t(ctx, "detect", 8.0 * (double)N * b);
+        launch_detect(ctx, dplan, g, psi, b, first, outputs_dev, weight, 1.0f);
+    }
+}
+}  // namespace
+
+void scan_device(Context& ctx, const simk_probe& probe, const std::vector<PotentialImpl*>& pots, int n_pos,
+                 const double* positions_dev, int n_det, const simk_detector* dets, double* const* outputs_dev) {
+    SIMK_REQUIRE(!pots.empty(), "no potential");
+    const GridGeom g = pots[0]->g;
+    for (auto* p : pots)
+        SIMK_REQUIRE(p->g.nx == g.nx && p->g.ny == g.ny &&
+                         std::fabs(p->g.ex - g.ex) <= 1e-12 * std::max(std::fabs(p->g.ex), std::fabs(g.ex)) &&
+                         std::fabs(p->g.ey - g.ey) <= 1e-12 * std::max(std::fabs(p->g.ey), std::fabs(g.ey)),
+                     "the potentials' grids must match the probe's");
+    const long long N = g.count();
+    auto dplan = build_detector_plan(ctx, g, probe.energy, dets, n_det);
+    for (int d = 0; d < n_det; ++d)
+        SIMK_CUDA(cudaMemsetAsync(outputs_dev[d], 0, (size_t)n_pos * dplan->det_count[d] * sizeof(double), ctx.stream));
+    DeviceBuffer spectrum;
+    probe_spectrum_device(ctx, g, probe, spectrum, nullptr);
+    const long long B = batch_size(ctx, g, n_pos);
+    ctx.work_a.ensure(B * N * sizeof(float2));
+    ctx.rx.ensure(B * g.nx * sizeof(float2));
+    ctx.ry.ensure(B * g.ny * sizeof(float2));
+    const double weight = 1.0 / (double)pots.size();
+    for (auto* pot : pots) {
+        prepare_transmissions(ctx, *pot, probe.energy);
+        bool fused = (ctx.form != SIMK_FORM_PLAIN) && fused_supported(ctx, g);
+        if (fused) ctx.work_b.ensure(B * N * sizeof(float2));
+        for (long long first = 0; first < n_pos; first += B) {
+            const int b = (int)std::min<long long>(B, n_pos - first);
+            if (fused)
+                scan_fused_batch(ctx, *pot, probe, spectrum.as<float2>(), positions_dev, first, b, *dplan, outputs_dev,
+                                 weight);
+            else
+                scan_plain_batch(ctx, *pot, probe, spectrum.as<float2>(), positions_dev, first, b, *dplan, outputs_dev,
+                                 weight);
+        }
+    }
+}
+
+}  // namespace simk

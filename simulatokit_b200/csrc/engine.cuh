@@ -1,0 +1,22 @@
+// engine.cuh -- entry points of the multislice engine (engine.cu) and of its fused form (fused.cu).
+#pragma once
+
+#include <functional>
+
+#include "context.cuh"
+
+namespace simk {
+
+long long batch_size(const Context& ctx, const GridGeom& g, long long count);
+void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, int count, const double* in_re,
+               const double* in_im, const std::vector<int>& planes, double* out_re, double* out_im);
+void scan_device(Context& ctx, const simk_probe& probe, const std::vector<PotentialImpl*>& pots, int n_pos,
+                 const double* positions_dev, int n_det, const simk_detector* dets, double* const* outputs_dev);
+
+// fused form (fused.cu)
+bool fused_supported(Context& ctx, const GridGeom& g);
+void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
+                      double* const* outputs_dev, double weight);
+
+}  // namespace simk

@@ -1,0 +1,139 @@
+"""Detectors and the STEM driver on the CUDA backend (Sources/SimulatoDetector/Detectors.swift, STEM.swift).
+
+Every detector runs on the device on |FFT2(exit)|^2 of each position, accumulated in float64, averaged over the
+potentials (frozen-phonon configurations)."""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .core import Grid, _refuse
+from .engine import Engine, ExecutionOptions
+from .multislice import Backend
+
+
+class AnnularDetector:
+    """sum P over inner^2 <= alpha^2 < outer^2 [mrad]; outer None: floor(min cutoff angles) (Detectors.swift:91-136)."""
+
+    def __init__(self, inner: float = 0.0, outer: float | None = None):
+        if not (math.isfinite(inner) and inner >= 0):
+            _refuse("inner must be finite and >= 0")
+        if outer is not None and not (math.isfinite(outer) and outer >= inner):
+            _refuse(f"outer must be finite and >= inner, got {outer}")
+        self.inner, self.outer = float(inner), outer
+
+    def c(self):
+        return L.Detector_t(L.DET_ANNULAR, 0, 0, 0 if self.outer is None else 1, 0, 0, self.inner,
+                            0.0 if self.outer is None else float(self.outer), 0.0)
+
+
+_MAX_ANGLE = {"cutoff": L.MAXANGLE_CUTOFF, "valid": L.MAXANGLE_VALID, "full": L.MAXANGLE_FULL}
+
+
+class PixelatedDetector:
+    """The pattern cropped (cutoff / valid / full) and fftshifted (Detectors.swift:140-168)."""
+
+    def __init__(self, max_angle: str = "valid"):
+        if max_angle not in _MAX_ANGLE:
+            _refuse(f"unknown max angle {max_angle!r}")
+        self.max_angle = max_angle
+
+    def c(self):
+        return L.Detector_t(L.DET_PIXELATED, _MAX_ANGLE[self.max_angle], 0, 0, 0, 0, 0.0, 0.0, 0.0)
+
+
+class CenterOfMassDetector:
+    """sum P alpha over a pixelated region, not divided by sum P; units "mrad" or "inverse" (Detectors.swift:172-206)."""
+
+    def __init__(self, max_angle: str = "valid", units: str = "inverse"):
+        if max_angle not in _MAX_ANGLE or units not in ("mrad", "inverse"):
+            _refuse("unknown max angle or units")
+        self.max_angle, self.units = max_angle, units
+
+    def c(self):
+        u = L.UNITS_MRAD if self.units == "mrad" else L.UNITS_INV_ANGSTROM
+        return L.Detector_t(L.DET_COM, _MAX_ANGLE[self.max_angle], u, 0, 0, 0, 0.0, 0.0, 0.0)
+
+
+class SegmentedDetector:
+    """n_r x n_phi polar bins between inner and outer [mrad], azimuth from rotation [rad] (Detectors.swift:210-263)."""
+
+    def __init__(self, radial_bins: int, azimuthal_bins: int, inner: float, outer: float, rotation: float = 0.0):
+        if radial_bins < 1 or azimuthal_bins < 1:
+            _refuse("bins must be at least 1")
+        if not (math.isfinite(inner) and math.isfinite(outer) and inner >= 0 and outer > inner
+                and math.isfinite(rotation)):
+            _refuse("need 0 <= inner < outer, finite, and a finite rotation")
+        self.nr, self.nphi, self.inner, self.outer, self.rotation = radial_bins, azimuthal_bins, inner, outer, rotation
+
+    def c(self):
+        return L.Detector_t(L.DET_SEGMENTED, 0, 0, 1, self.nr, self.nphi, float(self.inner), float(self.outer),
+                            float(self.rotation))
+
+
+def detector_shape(detector, grid: Grid, energy: float):
+    g = grid.c()
+    d = detector.c()
+    nd = C.c_int32(0)
+    sh = (C.c_int32 * 2)()
+    L.check(L.lib().simk_detector_shape(C.byref(g), energy, C.byref(d), C.byref(nd), sh))
+    return [] if nd.value == 0 else [sh[0]] if nd.value == 1 else [sh[0], sh[1]]
+
+
+@dataclass
+class ScanMeasurement:
+    """One detector's values over a scan, row-major (scan x, scan y, value shape) (STEM.swift:14-43)."""
+    scan_shape: list
+    value_shape: list
+    values: np.ndarray
+
+    def __getitem__(self, ixy):
+        ix, iy = ixy
+        n = int(np.prod(self.value_shape)) if self.value_shape else 1
+        base = (ix * self.scan_shape[1] + iy) * n
+        return self.values.reshape(-1)[base:base + n]
+
+    def array(self) -> np.ndarray:
+        return self.values.reshape(tuple(self.scan_shape) + tuple(self.value_shape))
+
+
+class STEM:
+    """STEM.scan (STEM.swift:49-150) on the device."""
+
+    @staticmethod
+    def scan(probe, potentials, scan, detectors, backend: Backend = Backend.cuda,
+             options: ExecutionOptions | None = None, engine: Engine | None = None):
+        if not potentials:
+            _refuse("no potential")
+        for p in potentials:
+            if not p.grid.matches(probe.grid):
+                _refuse("grid mismatch")
+        positions = np.ascontiguousarray(scan.positions, dtype=np.float64)
+        shape = list(scan.shape)
+        if not (1 <= len(shape) <= 2) or int(np.prod(shape)) != len(positions):
+            _refuse("the scan shape must have one or two axes whose product is the number of positions")
+        e = engine or Engine.require()
+        e.apply(options)
+        shapes = [detector_shape(d, probe.grid, probe.beam.energy) for d in detectors]
+        counts = [int(np.prod(s)) if s else 1 for s in shapes]
+        outs = [np.zeros(len(positions) * c) for c in counts]
+        handles = [p.handle(e) for p in potentials]
+        harr = (C.c_void_p * len(handles))(*[h.handle for h in handles])
+        darr = (L.Detector_t * max(1, len(detectors)))(*[d.c() for d in detectors])
+        oarr = (L.PD * max(1, len(outs)))(*[L.dptr(o) for o in outs])
+        p = probe.c()
+        L.check(e.lib.simk_scan(e.handle, C.byref(p), len(handles), harr, len(positions), L.dptr(positions),
+                                len(detectors), darr, oarr))
+        return [ScanMeasurement(shape, s, o) for s, o in zip(shapes, outs)]
+
+    @staticmethod
+    def scanFrozenPhonons(probe, phonons, nx, ny, slice_thickness, scan, detectors, parameterization=None,
+                          options: ExecutionOptions | None = None, engine: Engine | None = None):
+        """The scan averaged over every configuration of a FrozenPhonons ensemble."""
+        pots = phonons.lazy_potentials(nx, ny, slice_thickness, parameterization)
+        return STEM.scan(probe, pots, scan, detectors, options=options, engine=engine)
