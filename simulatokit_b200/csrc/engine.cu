@@ -69,10 +69,19 @@ void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, doubl
         SIMK_CUDA(cudaMemcpyAsync(ctx.work_a.ptr, host.data(), b * N * sizeof(float2), cudaMemcpyHostToDevice,
                                   ctx.stream));
         float2* psi = ctx.work_a.as<float2>();
+        const bool fused = (ctx.form != SIMK_FORM_PLAIN) && fused_supported(ctx, g);
+        if (fused) ctx.work_b.ensure(B * N * sizeof(float2));
         auto copy_out = [&](int j) {
             for (int q = 0; q < np; ++q) {
                 if (planes[q] != j) continue;
-                SIMK_CUDA(cudaMemcpyAsync(host.data(), psi, b * N * sizeof(float2), cudaMemcpyDeviceToHost, ctx.stream));
+                const float2* src = psi;
+                if (fused) {  // complete the row inverse transform on a copy
+                    SIMK_CUDA(cudaMemcpyAsync(ctx.work_b.ptr, psi, b * N * sizeof(float2), cudaMemcpyDeviceToDevice,
+                                              ctx.stream));
+                    finish_rows(ctx, g, ctx.work_b.as<float2>(), b);
+                    src = ctx.work_b.as<float2>();
+                }
+                SIMK_CUDA(cudaMemcpyAsync(host.data(), src, b * N * sizeof(float2), cudaMemcpyDeviceToHost, ctx.stream));
                 SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
                 // output layout: [wave][plane][N] for run (count = 1) and [wave][N] for run_batch (one plane)
                 for (int w = 0; w < b; ++w)
@@ -83,7 +92,10 @@ void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, doubl
                     }
             }
         };
-        propagate_plain(ctx, pot, energy, tx, ty, psi, b, true, copy_out);
+        if (fused)
+            propagate_fused(ctx, pot, energy, tx, ty, psi, b, false, [&](int j, bool) { copy_out(j); }, false);
+        else
+            propagate_plain(ctx, pot, energy, tx, ty, psi, b, true, copy_out);
     }
     SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
 }

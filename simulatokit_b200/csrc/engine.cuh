@@ -15,6 +15,12 @@ void scan_device(Context& ctx, const simk_probe& probe, const std::vector<Potent
 
 // fused form (fused.cu)
 bool fused_supported(Context& ctx, const GridGeom& g);
+// Every slice on `count` waves in place. probe_rows_pending: the waves come from the probe's column IFFT and still
+// need the row IFFT (and 1/N). After slice j the waves are in row-spectrum form (finish_rows completes them);
+// kspace_last: the last slice ends in k-space (P Phi) for the detectors. on_slice(j, kspace) after each slice.
+void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
+                     bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last);
+void finish_rows(Context& ctx, const GridGeom& g, float2* psi, int count);
 void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
                       const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
                       double* const* outputs_dev, double weight);

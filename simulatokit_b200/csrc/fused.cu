@@ -1,13 +1,378 @@
-// fused.cu -- the fused, batched form of the multislice step (register-resident FFT passes).
+// fused.cu -- the fused, batched form of the multislice step.
+//
+// One slice of every wave of a batch is two passes over HBM (32 N bytes per probe.slice step):
+//   row pass    (along y, contiguous):  [row IFFT] -> x t_j (x scale) -> [row FFT]
+//   column pass (along x, stride ny):   column FFT -> x P(dz_j) / N -> column IFFT      (slices 0 .. S-2)
+//                                       column FFT -> x P(dz_j)     -> store k-space     (the last slice)
+// The probe is generated inside the first column pass (Psi0 . r_x . r_y -> column IFFT) and the detectors read the
+// last column pass's k-space wave: FFT2(IFFT2(P Phi)) = P Phi, so |FFT2(exit)|^2 = |P Phi|^2 without two transforms.
+//
+// Each line transform is register-resident: with E elements per thread and T = n / E threads per line, thread t holds
+// elements t + T i (i < E). A Stockham pass of radix R (R | E) then reads its butterfly inputs from the thread's own
+// registers, and the last pass writes them back to the same slots, so a transform of P passes exchanges data through
+// shared memory P - 1 times. Loads and stores of t + T i are coalesced along rows; columns are read as tiles of TC
+// neighbouring columns so that consecutive threads read consecutive addresses.
+#include <algorithm>
+
 #include "engine.cuh"
 
 namespace simk {
 
-bool fused_supported(Context&, const GridGeom&) { return false; }
+constexpr int kMaxRegPasses = 12;
+// Threads per CTA by elements per thread, so that the register file holds E complex values per thread unspilled.
+constexpr int cols_threads(int E) { return E <= 8 ? 1024 : (E <= 12 ? 512 : 256); }
+constexpr int rows_threads(int E) { return E <= 12 ? 512 : 256; }
 
-void scan_fused_batch(Context&, PotentialImpl&, const simk_probe&, const float2*, const double*, long long, int,
-                      const DetectorPlan&, double* const*, double) {
-    throw Error(SIMK_ERR_INVALID, "fused form not available for this grid");
+struct RegPlan {
+    int n, E, T, npass;
+    int fac[kMaxRegPasses];
+    const float2* tw;  // n entries e^{-2 pi i k / n}
+};
+
+// Shared-memory slot of element idx of a line: rows pad one float2 per 16 (no bank conflicts on the strided
+// scatter); column tiles interleave the TC columns of the tile.
+struct SmemLine {
+    float2* base;
+    int stride;  // 1 for rows (padded), TC for column tiles
+    __device__ __forceinline__ float2& at(int idx) const {
+        return stride == 1 ? base[idx + (idx >> 4)] : base[idx * stride];
+    }
+};
+
+// ---- one register pass ----------------------------------------------------------------------------------------------
+// Butterflies jj = t + T q (q < E/R) on v[q + r E/R]; with `scatter`, the outputs go to their Stockham positions
+// (jj - k) R + k + r Ns in shared memory, k = jj mod Ns.
+template <int E, int R, int DIR>
+__device__ __forceinline__ void reg_pass(float2 (&v)[E], int t, int T, int Ns, int n, const float2* __restrict__ tw,
+                                         const SmemLine& sm, bool scatter) {
+    constexpr int Q = E / R;
+    const int tstride = n / (Ns * R);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        float2 u[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r] = v[q + r * Q];
+        const int jj = t + T * q;
+        const int k = jj % Ns;
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const float2 w = __ldg(tw + k * r * tstride);
+                u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
+            }
+        }
+        if (R == 2) bfly2<DIR>(u);
+        else if (R == 3) bfly3<DIR>(u);
+        else if (R == 4) bfly4<DIR>(u);
+        else if (R == 5) bfly5<DIR>(u);
+        else if (R == 8) bfly8<DIR>(u);
+        else if (R == 16) bfly16<DIR>(u);
+        if (scatter) {
+            const int o = (jj - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm.at(o + r * Ns) = u[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[q + r * Q] = u[r];
+        }
+    }
+}
+
+template <int E, int DIR>
+__device__ __forceinline__ void reg_pass_any(float2 (&v)[E], int R, int t, int T, int Ns, int n,
+                                             const float2* __restrict__ tw, const SmemLine& sm, bool scatter) {
+    switch (R) {
+        case 2: if constexpr (E % 2 == 0) reg_pass<E, 2, DIR>(v, t, T, Ns, n, tw, sm, scatter); break;
+        case 3: if constexpr (E % 3 == 0) reg_pass<E, 3, DIR>(v, t, T, Ns, n, tw, sm, scatter); break;
+        case 4: if constexpr (E % 4 == 0) reg_pass<E, 4, DIR>(v, t, T, Ns, n, tw, sm, scatter); break;
+        case 5: if constexpr (E % 5 == 0) reg_pass<E, 5, DIR>(v, t, T, Ns, n, tw, sm, scatter); break;
+        case 8: if constexpr (E % 8 == 0) reg_pass<E, 8, DIR>(v, t, T, Ns, n, tw, sm, scatter); break;
+        case 16: if constexpr (E % 16 == 0) reg_pass<E, 16, DIR>(v, t, T, Ns, n, tw, sm, scatter); break;
+        default: break;
+    }
+}
+
+// The whole transform of one line held as v[i] = x[t + T i]; result in the same layout.
+template <int E, int DIR>
+__device__ __forceinline__ void reg_fft(float2 (&v)[E], int t, const RegPlan& p, const SmemLine& sm) {
+    const int T = p.T;
+    int Ns = 1;
+    for (int f = 0; f < p.npass; ++f) {
+        const int R = p.fac[f];
+        const bool scatter = (f + 1 < p.npass);
+        reg_pass_any<E, DIR>(v, R, t, T, Ns, p.n, p.tw, sm, scatter);
+        if (scatter) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < E; ++i) v[i] = sm.at(t + T * i);
+            __syncthreads();
+        }
+        Ns *= R;
+    }
+}
+
+// ---- row pass -------------------------------------------------------------------------------------------------------
+// rows r = (wave, ix) of `count` waves; RB rows per CTA (blockDim = (T, RB)).
+template <int E>
+__global__ void __launch_bounds__(rows_threads(E)) fused_rows_kernel(float2* __restrict__ psi, const float2* __restrict__ tmul,
+                                                         RegPlan p, int nx, long long nrows, int inv, int fwd,
+                                                         float scale) {
+    extern __shared__ __align__(16) float2 smem_rows[];
+    const int t = threadIdx.x;
+    const int rr = threadIdx.y;
+    const int ny = p.n;
+    const int lds = ny + ny / 16 + 1;
+    SmemLine sm{smem_rows + rr * lds, 1};
+    const long long r = (long long)blockIdx.x * blockDim.y + rr;
+    const bool active = r < nrows;
+    const long long rc = active ? r : nrows - 1;  // inactive rows recompute the last row and do not store
+    float2* row = psi + rc * ny;
+    float2 v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = row[t + p.T * i];
+    if (inv) reg_fft<E, +1>(v, t, p, sm);
+    if (tmul) {
+        const int ix = (int)(rc % nx);
+        const float2* tr = tmul + (long long)ix * ny;
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = cmul(v[i], __ldg(tr + t + p.T * i)) * scale;
+    } else if (scale != 1.0f) {
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = v[i] * scale;
+    }
+    if (fwd) reg_fft<E, -1>(v, t, p, sm);
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < E; ++i) row[t + p.T * i] = v[i];
+    }
+}
+
+// ---- column pass ----------------------------------------------------------------------------------------------------
+// mode 0: FFT -> x P * pscale -> IFFT;  mode 1: FFT -> x P * pscale (k-space out);  mode 2: probe spectrum -> IFFT.
+// blockDim = (TC, T); grid = (ny / TC, count).
+struct ColArgs {
+    float2* psi;
+    const float2* P;
+    float pscale;
+    int mode;
+    int ny;
+    const float2* spectrum;
+    const float2* rx;
+    const float2* ry;
+};
+
+template <int E>
+__global__ void __launch_bounds__(cols_threads(E)) fused_cols_kernel(ColArgs a, RegPlan p) {
+    extern __shared__ __align__(16) float2 smem_cols[];
+    const int c = threadIdx.x, TC = blockDim.x;
+    const int t = threadIdx.y;
+    const int nx = p.n, ny = a.ny;
+    const int iy = blockIdx.x * TC + c;
+    const long long b = blockIdx.y;
+    const long long N = (long long)nx * ny;
+    SmemLine sm{smem_cols + c, TC};
+    float2* col = a.psi + b * N + iy;
+    float2 v[E];
+    if (a.mode == 2) {
+        const float2 ryv = a.ry[b * ny + iy];
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const int ix = t + p.T * i;
+            v[i] = cmul(cmul(__ldg(a.spectrum + (long long)ix * ny + iy), __ldg(a.rx + b * nx + ix)), ryv);
+        }
+        reg_fft<E, +1>(v, t, p, sm);
+    } else {
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = col[(long long)(t + p.T * i) * ny];
+        reg_fft<E, -1>(v, t, p, sm);
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = cmul(v[i], __ldg(a.P + (long long)(t + p.T * i) * ny + iy)) * a.pscale;
+        if (a.mode == 0) reg_fft<E, +1>(v, t, p, sm);
+    }
+#pragma unroll
+    for (int i = 0; i < E; ++i) col[(long long)(t + p.T * i) * ny] = v[i];
+}
+
+// ---- plans and launches ---------------------------------------------------------------------------------------------
+namespace {
+
+bool factor_with(int n, int E, std::vector<int>& out) {
+    out.clear();
+    int rest = n;
+    for (int r : {16, 8, 4, 2, 5, 3}) {
+        if (E % r) continue;
+        while (rest % r == 0 && rest > 1) {
+            out.push_back(r);
+            rest /= r;
+        }
+    }
+    return rest == 1;
+}
+
+struct RegChoice {
+    int E = 0;
+    std::vector<int> fac;
+};
+
+RegChoice choose(int n) {
+    RegChoice best;
+    for (int E : {8, 16, 12, 20, 24}) {
+        std::vector<int> f;
+        if (n % E) continue;
+        const int T = n / E;
+        if (T < 4 || T > 256) continue;
+        if (!factor_with(n, E, f)) continue;
+        if ((int)f.size() > kMaxRegPasses) continue;
+        if (best.E == 0 || f.size() < best.fac.size()) {
+            best.E = E;
+            best.fac = f;
+        }
+    }
+    return best;
+}
+
+RegPlan reg_plan(Context& ctx, int n) {
+    RegChoice ch = choose(n);
+    SIMK_REQUIRE(ch.E != 0, "no register FFT plan for length " + std::to_string(n));
+    RegPlan p{};
+    p.n = n;
+    p.E = ch.E;
+    p.T = n / ch.E;
+    p.npass = (int)ch.fac.size();
+    for (int i = 0; i < p.npass; ++i) p.fac[i] = ch.fac[i];
+    p.tw = static_cast<const float2*>(ctx.plan(n, 32).tw.ptr);
+    return p;
+}
+
+template <int E>
+void launch_rows_e(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
+                   int fwd, float scale) {
+    const int RB = std::max(1, std::min(8, std::min(256, rows_threads(E)) / p.T));
+    SIMK_REQUIRE(RB * p.T <= rows_threads(E), "row tile too large");
+    const int lds = p.n + p.n / 16 + 1;
+    const size_t smem = (size_t)RB * lds * sizeof(float2);
+    static bool set = false;
+    if (!set) {
+        SIMK_CUDA(cudaFuncSetAttribute(fused_rows_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        set = true;
+    }
+    dim3 block(p.T, RB);
+    const long long blocks = (nrows + RB - 1) / RB;
+    fused_rows_kernel<E><<<(unsigned)blocks, block, smem, ctx.stream>>>(psi, tmul, p, nx, nrows, inv, fwd, scale);
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+}
+
+template <int E>
+void launch_cols_e(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    int TC = 16;
+    while (TC > 1 && (TC * p.T > cols_threads(E) || a.ny % TC)) TC /= 2;
+    SIMK_REQUIRE(TC * p.T <= cols_threads(E), "column tile too large");
+    const size_t smem = (size_t)TC * p.n * sizeof(float2);
+    static bool set = false;
+    if (!set) {
+        SIMK_CUDA(cudaFuncSetAttribute(fused_cols_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        set = true;
+    }
+    SIMK_REQUIRE(smem <= 160 * 1024, "column tile too large");
+    dim3 block(TC, p.T);
+    dim3 grid(a.ny / TC, count);
+    fused_cols_kernel<E><<<grid, block, smem, ctx.stream>>>(a, p);
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+}
+
+void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
+                 int fwd, float scale) {
+    KernelTimer timer(ctx, "fused_rows", 16.0 * (double)nrows * p.n);
+    switch (p.E) {
+        case 8: launch_rows_e<8>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+        case 12: launch_rows_e<12>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+        case 16: launch_rows_e<16>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+        case 20: launch_rows_e<20>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+        case 24: launch_rows_e<24>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+        default: throw Error(SIMK_ERR_INVALID, "unsupported register plan");
+    }
+}
+
+void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    const double bytes = (a.mode == 2 ? 8.0 : 16.0) * (double)p.n * a.ny * count;
+    KernelTimer timer(ctx, "fused_cols", bytes);
+    switch (p.E) {
+        case 8: launch_cols_e<8>(ctx, p, a, count); break;
+        case 12: launch_cols_e<12>(ctx, p, a, count); break;
+        case 16: launch_cols_e<16>(ctx, p, a, count); break;
+        case 20: launch_cols_e<20>(ctx, p, a, count); break;
+        case 24: launch_cols_e<24>(ctx, p, a, count); break;
+        default: throw Error(SIMK_ERR_INVALID, "unsupported register plan");
+    }
+}
+
+}  // namespace
+
+bool fused_supported(Context&, const GridGeom& g) { return choose(g.nx).E != 0 && choose(g.ny).E != 0; }
+
+void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
+                     bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    const RegPlan prow = reg_plan(ctx, g.ny);
+    const RegPlan pcol = reg_plan(ctx, g.nx);
+    const int S = pot.n_slices();
+    const float invN = 1.0f / (float)N;
+    for (int j = 0; j < S; ++j) {
+        // rows: complete the previous inverse transform (or the probe's), x t_j, forward
+        const bool inv = (j > 0) || probe_rows_pending;
+        const float rscale = (j == 0 && probe_rows_pending) ? invN : 1.0f;
+        launch_rows(ctx, prow, psi, pot.t.as<float2>() + (long long)j * N, g.nx, (long long)count * g.nx, inv ? 1 : 0,
+                    1, rscale);
+        const Propagator& P = ctx.propagator(g, energy, pot.dz[j], tx, ty);
+        const bool last = (j == S - 1);
+        ColArgs a{};
+        a.psi = psi;
+        a.P = P.p.as<float2>();
+        a.ny = g.ny;
+        if (last && kspace_last) {
+            a.mode = 1;
+            a.pscale = 1.0f;
+        } else {
+            a.mode = 0;
+            a.pscale = invN;
+        }
+        launch_cols(ctx, pcol, a, count);
+        if (on_slice) on_slice(j, last && kspace_last);
+    }
+}
+
+// The waves after slice j are in "row spectrum" form (columns inverse-transformed, rows not): the row IFFT that
+// completes them, in place.
+void finish_rows(Context& ctx, const GridGeom& g, float2* psi, int count) {
+    const RegPlan prow = reg_plan(ctx, g.ny);
+    launch_rows(ctx, prow, psi, nullptr, g.nx, (long long)count * g.nx, 1, 0, 1.0f);
+}
+
+void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
+                      double* const* outputs_dev, double weight) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    float2* psi = ctx.work_a.as<float2>();
+    launch_ramps(ctx, g, positions_dev, first, b, ctx.rx.as<float2>(), ctx.ry.as<float2>());
+    const RegPlan pcol = reg_plan(ctx, g.nx);
+    ColArgs a{};
+    a.psi = psi;
+    a.mode = 2;
+    a.ny = g.ny;
+    a.spectrum = spectrum;
+    a.rx = ctx.rx.as<float2>();
+    a.ry = ctx.ry.as<float2>();
+    a.pscale = 1.0f;
+    launch_cols(ctx, pcol, a, b);
+    propagate_fused(ctx, pot, probe.energy, probe.tilt_x, probe.tilt_y, psi, b, true, nullptr, true);
+    {
+        KernelTimer t(ctx, "detect", 8.0 * (double)N * b);
+        launch_detect(ctx, dplan, g, psi, b, first, outputs_dev, weight, 1.0f);
+    }
 }
 
 }  // namespace simk
