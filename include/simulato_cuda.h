@@ -165,6 +165,18 @@ int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_poten
                      simk_potential* const* potentials, int32_t n_positions, const double* positions_xy_device,
                      int32_t n_detectors, const simk_detector* detectors, double* const* outputs_device);
 
+/* ---- no-allocation variant ---------------------------------------------------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot let the library allocate device memory
+ * (a host framework that owns all device memory through its own allocator, such as PyTorch's caching allocator or an
+ * XLA custom call, where a cudaMalloc inside the call would bypass its accounting and may synchronise the device).
+ * Writes Probe.centredSpectrum (the same values as simk_probe_spectrum, rounded to complex64, interleaved re, im,
+ * nx x ny) into the caller's device buffer `out_device`, on `stream` (a cudaStream_t; NULL = the default stream),
+ * without synchronising. It allocates nothing: its scratch is a fixed 32 KiB float64 array in the library's device
+ * image, so grids above 2048 x 2048 pixels (4,194,304) are refused with SIMK_ERR_INVALID. The first call on a device
+ * (with that device current) looks up the array's address; make it before any stream capture. Every call shares the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. */
+int simk_probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void* out_device, void* stream);
+
 /* ---- the transform itself (FFT2D, Sources/SimulatoCore/FFT2D.swift:169-265) ----------------------------------------
  * `count` nx x ny fields, forward (unnormalised, e^{-2 pi i}) or inverse (x 1/(nx ny)), in float32 (precision 32) or
  * float64 (precision 64) on the device. A test hook: the hot path calls the transforms internally. */

@@ -29,7 +29,7 @@ EXPORTED = [
     "simk_context_launch_count", "simk_context_kernel_time", "simk_potential_from_atoms", "simk_potential_from_values", "simk_potential_destroy",
     "simk_potential_slice_count", "simk_potential_read_slices", "simk_potential_read_transmission", "simk_run",
     "simk_run_batch", "simk_probe_spectrum", "simk_build_probes", "simk_detector_shape", "simk_scan",
-    "simk_scan_device", "simk_fft2",
+    "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc",
 ]
 
 
@@ -103,6 +103,7 @@ def _signatures(lib):
         "simk_scan_device": [P, C.POINTER(Probe_t), i32, C.POINTER(P), i32, P, i32, C.POINTER(Detector_t),
                              C.POINTER(P)],
         "simk_fft2": [P, i32, i32, i32, i32, i32, PD, PD, PD, PD],
+        "simk_probe_spectrum_noalloc": [C.POINTER(Grid_t), C.POINTER(Probe_t), P, P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

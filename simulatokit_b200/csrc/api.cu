@@ -8,6 +8,10 @@
 
 using namespace simk;
 
+namespace simk {
+void probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void* out_device, void* stream);
+}
+
 namespace {
 thread_local std::string g_last_error;
 
@@ -472,6 +476,10 @@ int simk_fft2(simk_context* ctx, int32_t nx, int32_t ny, int32_t count, int32_t 
             }
         }
     });
+}
+
+int simk_probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void* out_device, void* stream) {
+    return guarded([&] { probe_spectrum_noalloc(grid, probe, out_device, stream); });
 }
 
 }  // extern "C"
