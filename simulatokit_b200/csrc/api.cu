@@ -131,7 +131,15 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
             case SIMK_OPT_BATCH: SIMK_REQUIRE(value >= 0, "batch must be >= 0"); c.batch = value; break;
             case SIMK_OPT_BATCH_BYTES: c.batch_bytes = std::max<int64_t>(1, value); break;
             case SIMK_OPT_GRAPHS: c.graphs = value ? 1 : 0; break;
-            case SIMK_OPT_TIMING: c.timing = value ? 1 : 0; break;
+            case SIMK_OPT_TIMING:
+                c.timing = value ? 1 : 0;
+                if (c.timing) c.times.reserve(16384);
+                break;
+            case SIMK_OPT_COL_TILE:
+                SIMK_REQUIRE(value == 0 || value == 1 || value == 2 || value == 4 || value == 8 || value == 16,
+                             "column tile must be 0, 1, 2, 4, 8 or 16");
+                c.col_tile = (int)value;
+                break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -169,6 +177,7 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_BATCH_BYTES: *value = c.batch_bytes; break;
             case SIMK_OPT_GRAPHS: *value = c.graphs; break;
             case SIMK_OPT_TIMING: *value = c.timing; break;
+            case SIMK_OPT_COL_TILE: *value = c.col_tile; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });

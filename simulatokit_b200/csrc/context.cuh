@@ -58,6 +58,14 @@ struct KernelTimes {
     std::map<std::string, std::vector<Rec>> pending;
     std::map<std::string, std::tuple<double, long long, double>> done;  // ms, launches, bytes
     std::vector<cudaEvent_t> pool;
+    // Creates `n` events up front so that recording them in the hot loop costs no cudaEventCreate.
+    void reserve(size_t n) {
+        while (pool.size() < n) {
+            cudaEvent_t e;
+            SIMK_CUDA(cudaEventCreate(&e));
+            pool.push_back(e);
+        }
+    }
     cudaEvent_t get() {
         if (!pool.empty()) {
             cudaEvent_t e = pool.back();
@@ -104,12 +112,16 @@ struct Context {
     long long batch = 0;
     long long batch_bytes = 1LL << 30;
     int graphs = 1;
+    int col_tile = 0;
     int64_t launches = 0;
     std::map<std::pair<int, int>, std::unique_ptr<LinePlan>> plans;
     std::map<std::tuple<int, int, double, double, double, double, double, double>, std::unique_ptr<Propagator>> props;
     // workspaces
     DeviceBuffer work_a, work_b, work_c, rx, ry, positions, partial;
     std::vector<DeviceBuffer> outputs;
+    // per-scan set-up kept across calls: detector maps by (grid, energy, detectors), spectra by (grid, probe)
+    std::map<std::string, std::unique_ptr<DetectorPlan>> detector_plans;
+    std::map<std::string, std::unique_ptr<DeviceBuffer>> spectra;
 
     const LinePlan& plan(int n, int precision) {
         auto key = std::make_pair(n, precision);

@@ -132,11 +132,29 @@ void scan_device(Context& ctx, const simk_probe& probe, const std::vector<Potent
                          std::fabs(p->g.ey - g.ey) <= 1e-12 * std::max(std::fabs(p->g.ey), std::fabs(g.ey)),
                      "the potentials' grids must match the probe's");
     const long long N = g.count();
-    auto dplan = build_detector_plan(ctx, g, probe.energy, dets, n_det);
+    // detector maps and the probe spectrum depend only on (grid, energy, detectors) and (grid, probe): built once
+    auto key_bytes = [](const void* p, size_t n) { return std::string(static_cast<const char*>(p), n); };
+    std::string gkey = key_bytes(&g.nx, sizeof(int) * 2) + key_bytes(&g.ex, sizeof(double)) +
+                       key_bytes(&g.ey, sizeof(double));
+    std::string dkey = gkey + key_bytes(&probe.energy, sizeof(double)) +
+                       key_bytes(dets, sizeof(simk_detector) * (size_t)n_det);
+    auto dit = ctx.detector_plans.find(dkey);
+    if (dit == ctx.detector_plans.end()) {
+        if (ctx.detector_plans.size() > 64) ctx.detector_plans.clear();
+        dit = ctx.detector_plans.emplace(dkey, build_detector_plan(ctx, g, probe.energy, dets, n_det)).first;
+    }
+    const DetectorPlan* dplan = dit->second.get();
+    std::string skey = gkey + key_bytes(&probe, sizeof(simk_probe));
+    auto sit = ctx.spectra.find(skey);
+    if (sit == ctx.spectra.end()) {
+        if (ctx.spectra.size() > 64) ctx.spectra.clear();
+        auto buf = std::make_unique<DeviceBuffer>();
+        probe_spectrum_device(ctx, g, probe, *buf, nullptr);
+        sit = ctx.spectra.emplace(skey, std::move(buf)).first;
+    }
+    const DeviceBuffer& spectrum = *sit->second;
     for (int d = 0; d < n_det; ++d)
         SIMK_CUDA(cudaMemsetAsync(outputs_dev[d], 0, (size_t)n_pos * dplan->det_count[d] * sizeof(double), ctx.stream));
-    DeviceBuffer spectrum;
-    probe_spectrum_device(ctx, g, probe, spectrum, nullptr);
     const long long B = batch_size(ctx, g, n_pos);
     ctx.work_a.ensure(B * N * sizeof(float2));
     ctx.rx.ensure(B * g.nx * sizeof(float2));

@@ -193,6 +193,164 @@ __global__ void __launch_bounds__(cols_threads(E)) fused_cols_kernel(ColArgs a, 
     for (int i = 0; i < E; ++i) col[(long long)(t + p.T * i) * ny] = v[i];
 }
 
+// ---- compile-time plans for n = 2^L -----------------------------------------------------------------------------------
+// E = 8 elements per thread, T = n / 8 threads per line, radix-8 passes then one radix-2 or radix-4 pass when L is not a
+// multiple of 3. Every Ns, twiddle stride and shared-memory offset is a compile-time constant, each thread's twiddles
+// (the same for every transform it runs) are loaded once into registers, and shared memory is addressed through the
+// swizzle idx ^ ((idx >> 3) & 15), which makes every scatter and gather of these plans free of bank conflicts.
+constexpr int ct_log2(int n) { return n <= 1 ? 0 : 1 + ct_log2(n / 2); }
+template <int N> struct Pow2 {
+    static constexpr int L = ct_log2(N);
+    static constexpr int T = N / 8;
+    static constexpr int NP = (L + 2) / 3;
+    static constexpr int radix(int f) { return (f < L / 3) ? 8 : (1 << (L % 3)); }
+    static constexpr int ns(int f) { return f == 0 ? 1 : ns(f - 1) * radix(f - 1); }
+};
+
+__device__ __forceinline__ int swz(int idx) { return idx ^ ((idx >> 3) & 15); }
+
+// Element idx of a line in shared memory: rows (STRIDE 0) contiguous, column tiles interleave STRIDE columns.
+template <int STRIDE> struct SmemCT {
+    float2* base;
+    __device__ __forceinline__ float2& at(int idx) const {
+        if constexpr (STRIDE == 0) return base[swz(idx)];
+        else return base[swz(idx) * STRIDE];
+    }
+};
+
+// Per-thread twiddles: pass f >= 1 uses w[f - 1][q (R - 1) + r - 1] = W_n^{k r n / (Ns R)}, k = (t + T q) mod Ns.
+template <int N> struct TwRegs {
+    float2 w[Pow2<N>::NP > 1 ? Pow2<N>::NP - 1 : 1][7];
+};
+
+template <int N, int F>
+__device__ __forceinline__ void tw_load(TwRegs<N>& tr, unsigned t, const float2* __restrict__ tw) {
+    using P = Pow2<N>;
+    if constexpr (F < P::NP) {
+        constexpr int R = P::radix(F), NS = P::ns(F), Q = 8 / R, TSTRIDE = N / (NS * R);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const unsigned k = (t + P::T * q) & (NS - 1);
+#pragma unroll
+            for (int r = 1; r < R; ++r) tr.w[F - 1][q * (R - 1) + r - 1] = __ldg(tw + k * (r * TSTRIDE));
+        }
+        tw_load<N, F + 1>(tr, t, tw);
+    }
+}
+
+template <int N, int F, int DIR, int STRIDE>
+__device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const TwRegs<N>& tr,
+                                            const SmemCT<STRIDE>& sm) {
+    using P = Pow2<N>;
+    if constexpr (F < P::NP) {
+        constexpr int R = P::radix(F), NS = P::ns(F), Q = 8 / R;
+        constexpr bool SC = (F + 1 < P::NP);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            float2 u[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) u[r] = v[q + r * Q];
+            if constexpr (F > 0) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const float2 w = tr.w[F - 1][q * (R - 1) + r - 1];
+                    u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
+                }
+            }
+            if constexpr (R == 2) bfly2<DIR>(u);
+            else if constexpr (R == 4) bfly4<DIR>(u);
+            else bfly8<DIR>(u);
+            if constexpr (SC) {
+                const int jj = (int)t + P::T * q;
+                const int k = jj & (NS - 1);
+                const int o = (jj - k) * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) sm.at(o + r * NS) = u[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[q + r * Q] = u[r];
+            }
+        }
+        if constexpr (SC) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = sm.at((int)t + P::T * i);
+            __syncthreads();
+        }
+        ct_fft_from<N, F + 1, DIR, STRIDE>(v, t, tr, sm);
+    }
+}
+
+// rows: blockDim = (N / 8, RB); row r = (wave, ix) of nrows = count * nx
+template <int N>
+__global__ void __launch_bounds__(256) fused_rows_ct(float2* __restrict__ psi, const float2* __restrict__ tmul,
+                                                     const float2* __restrict__ tw, unsigned nx, unsigned nrows,
+                                                     int inv, int fwd, float scale) {
+    extern __shared__ __align__(16) float2 smem_rows_ct[];
+    constexpr int T = N / 8;
+    const unsigned t = threadIdx.x;
+    const unsigned r = blockIdx.x * blockDim.y + threadIdx.y;
+    const bool active = r < nrows;
+    const unsigned rc = active ? r : nrows - 1;  // inactive rows recompute the last row and do not store
+    SmemCT<0> sm{smem_rows_ct + threadIdx.y * N};
+    TwRegs<N> tr;
+    tw_load<N, 1>(tr, t, tw);
+    float2* row = psi + (size_t)rc * N;
+    float2 v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = row[t + T * i];
+    if (inv) ct_fft_from<N, 0, +1>(v, t, tr, sm);
+    if (tmul) {
+        const float2* trow = tmul + (size_t)(rc % nx) * N;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], __ldg(trow + t + T * i)) * scale;
+    } else if (scale != 1.0f) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = v[i] * scale;
+    }
+    if (fwd) ct_fft_from<N, 0, -1>(v, t, tr, sm);
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
+    }
+}
+
+// columns: blockDim = (TC, N / 8), grid = (ny / TC, count). MODE 0: FFT -> x P pscale -> IFFT; 1: FFT -> x P pscale;
+// 2: probe spectrum Psi0 r_x r_y -> IFFT.
+template <int N, int TC, int MODE>
+__global__ void __launch_bounds__(TC * (N / 8)) fused_cols_ct(ColArgs a, const float2* __restrict__ tw) {
+    extern __shared__ __align__(16) float2 smem_cols_ct[];
+    constexpr int T = N / 8;
+    const int c = threadIdx.x;
+    const unsigned t = threadIdx.y;
+    const int ny = a.ny;
+    const int iy = blockIdx.x * TC + c;
+    const size_t b = blockIdx.y;
+    SmemCT<TC> sm{smem_cols_ct + c};
+    TwRegs<N> tr;
+    tw_load<N, 1>(tr, t, tw);
+    float2* col = a.psi + b * (size_t)N * ny + iy;
+    float2 v[8];
+    if constexpr (MODE == 2) {
+        const float2 ryv = a.ry[b * ny + iy];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int ix = (int)t + T * i;
+            v[i] = cmul(cmul(__ldg(a.spectrum + (size_t)ix * ny + iy), __ldg(a.rx + b * N + ix)), ryv);
+        }
+        ct_fft_from<N, 0, +1>(v, t, tr, sm);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = col[(size_t)(t + T * i) * ny];
+        ct_fft_from<N, 0, -1>(v, t, tr, sm);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], __ldg(a.P + (size_t)(t + T * i) * ny + iy)) * a.pscale;
+        if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, tr, sm);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
+}
+
 // ---- plans and launches ---------------------------------------------------------------------------------------------
 namespace {
 
@@ -282,9 +440,96 @@ void launch_cols_e(Context& ctx, const RegPlan& p, const ColArgs& a, int count) 
     ++ctx.launches;
 }
 
+template <int N>
+void launch_rows_ct(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
+                    int fwd, float scale) {
+    constexpr int T = N / 8;
+    constexpr int RB = (256 / T) > 0 ? (256 / T) : 1;
+    const size_t smem = (size_t)RB * N * sizeof(float2);
+    static bool set = false;
+    if (!set) {
+        SIMK_CUDA(cudaFuncSetAttribute(fused_rows_ct<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        set = true;
+    }
+    SIMK_REQUIRE(nrows < (1LL << 31), "too many rows in one batch");
+    dim3 block(T, RB);
+    const long long blocks = (nrows + RB - 1) / RB;
+    fused_rows_ct<N><<<(unsigned)blocks, block, smem, ctx.stream>>>(psi, tmul, p.tw, (unsigned)nx, (unsigned)nrows,
+                                                                    inv, fwd, scale);
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+}
+
+template <int N, int TC, int MODE>
+void launch_cols_ct_m(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    constexpr int T = N / 8;
+    const size_t smem = (size_t)TC * N * sizeof(float2);
+    static bool set = false;
+    if (!set) {
+        SIMK_CUDA(cudaFuncSetAttribute(fused_cols_ct<N, TC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       160 * 1024));
+        set = true;
+    }
+    dim3 block(TC, T);
+    dim3 grid(a.ny / TC, count);
+    fused_cols_ct<N, TC, MODE><<<grid, block, smem, ctx.stream>>>(a, p.tw);
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+}
+
+template <int N, int TC>
+void launch_cols_ct(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    switch (a.mode) {
+        case 0: launch_cols_ct_m<N, TC, 0>(ctx, p, a, count); break;
+        case 1: launch_cols_ct_m<N, TC, 1>(ctx, p, a, count); break;
+        default: launch_cols_ct_m<N, TC, 2>(ctx, p, a, count); break;
+    }
+}
+
+bool rows_ct(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv, int fwd,
+             float scale) {
+    switch (p.n) {
+        case 128: launch_rows_ct<128>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
+        case 256: launch_rows_ct<256>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
+        case 512: launch_rows_ct<512>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
+        case 1024: launch_rows_ct<1024>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
+        case 2048: launch_rows_ct<2048>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
+        default: return false;
+    }
+}
+
+template <int N>
+bool cols_ct_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
+    // TC x N/8 threads per CTA, at most 1024
+    if (tc * (N / 8) > 1024 || a.ny % tc) return false;
+    switch (tc) {
+        case 1: launch_cols_ct<N, 1>(ctx, p, a, count); return true;
+        case 2: launch_cols_ct<N, 2>(ctx, p, a, count); return true;
+        case 4: launch_cols_ct<N, 4>(ctx, p, a, count); return true;
+        case 8: if constexpr (8 * (N / 8) <= 1024) { launch_cols_ct<N, 8>(ctx, p, a, count); return true; } return false;
+        case 16: if constexpr (16 * (N / 8) <= 1024) { launch_cols_ct<N, 16>(ctx, p, a, count); return true; } return false;
+        default: return false;
+    }
+}
+
+// Column tile width: the context's SIMK_OPT_COL_TILE, else 4 columns (three CTAs per SM at 512).
+bool cols_ct(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    int tc = ctx.col_tile > 0 ? ctx.col_tile : 4;
+    while (tc > 1 && (a.ny % tc || tc * (p.n / 8) > 1024)) tc /= 2;
+    switch (p.n) {
+        case 128: return cols_ct_tc<128>(ctx, p, a, count, tc);
+        case 256: return cols_ct_tc<256>(ctx, p, a, count, tc);
+        case 512: return cols_ct_tc<512>(ctx, p, a, count, tc);
+        case 1024: return cols_ct_tc<1024>(ctx, p, a, count, tc);
+        case 2048: return cols_ct_tc<2048>(ctx, p, a, count, tc);
+        default: return false;
+    }
+}
+
 void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
                  int fwd, float scale) {
     KernelTimer timer(ctx, "fused_rows", 16.0 * (double)nrows * p.n);
+    if (rows_ct(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return;
     switch (p.E) {
         case 8: launch_rows_e<8>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
         case 12: launch_rows_e<12>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
@@ -298,6 +543,7 @@ void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul
 void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     const double bytes = (a.mode == 2 ? 8.0 : 16.0) * (double)p.n * a.ny * count;
     KernelTimer timer(ctx, "fused_cols", bytes);
+    if (cols_ct(ctx, p, a, count)) return;
     switch (p.E) {
         case 8: launch_cols_e<8>(ctx, p, a, count); break;
         case 12: launch_cols_e<12>(ctx, p, a, count); break;

@@ -17,17 +17,20 @@ class ExecutionOptions:
 
     form: "plain" (one operation per launch), "fused" (batched fused passes, the default) or "bf16x3" (fused with
     tensor-core DFT stages). batch: waves per batch (0 = from batch_bytes). batch_bytes: bytes of waves one batch
-    may hold (default 1 GiB). graphs: capture each batch's slice loop in a CUDA graph."""
+    may hold (default 1 GiB). graphs: capture each batch's slice loop in a CUDA graph. col_tile: columns per CTA of
+    the fused column pass (0 = automatic)."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
-    def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True):
+    def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
+                 col_tile: int = 0):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
         self.form = form
         self.batch = max(0, int(batch))
         self.batch_bytes = max(1, int(batch_bytes))
         self.graphs = bool(graphs)
+        self.col_tile = int(col_tile)
 
     @staticmethod
     def standard() -> "ExecutionOptions":
@@ -69,6 +72,7 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_BATCH, o.batch))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_BATCH_BYTES, o.batch_bytes))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_GRAPHS, 1 if o.graphs else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COL_TILE, o.col_tile))
 
     def set_stream(self, stream_ptr: int | None):
         L.check(self.lib.simk_context_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
