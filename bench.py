@@ -201,6 +201,7 @@ def main():
     ap.add_argument("--form", default="fused", choices=["plain", "fused", "bf16x3"])
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--col-tile", type=int, default=0)
+    ap.add_argument("--no-tma", action="store_true")
     ap.add_argument("--cpu-positions", type=int, default=32)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
@@ -230,7 +231,7 @@ def main():
     torch.cuda.set_stream(stream)
     assert stream.cuda_stream != 0
     engine.set_stream(stream.cuda_stream)
-    opts = sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile)
+    opts = sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma)
     engine.apply(opts)
 
     box, nums, pos = srtio3(8, 8, 20)
@@ -345,6 +346,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "form": args.form, "batch": args.batch, "col_tile": args.col_tile,
+                           "tma": not args.no_tma,
                            "positions": n_pos, "slices": 20,
                            "grid": [NX, NY], "replicas": world, "l2": "inputs larger than L2 (batch of waves up to "
                                                                      "1 GiB per launch)"},

@@ -140,6 +140,7 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                              "column tile must be 0, 1, 2, 4, 8 or 16");
                 c.col_tile = (int)value;
                 break;
+            case SIMK_OPT_TMA: c.tma = value ? 1 : 0; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -178,6 +179,7 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_GRAPHS: *value = c.graphs; break;
             case SIMK_OPT_TIMING: *value = c.timing; break;
             case SIMK_OPT_COL_TILE: *value = c.col_tile; break;
+            case SIMK_OPT_TMA: *value = c.tma; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -186,8 +188,10 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
 int simk_context_synchronize(simk_context* ctx) {
     return guarded([&] {
         SIMK_REQUIRE(ctx, "context is null");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
         activate(ctx->impl);
         SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+        check_device_error(ctx->impl);
     });
 }
 
@@ -430,6 +434,7 @@ int simk_scan(simk_context* ctx, const simk_probe* probe, int32_t n_potentials, 
             SIMK_CUDA(cudaMemcpyAsync(outputs[d], dev_out[d], n_positions * counts[d] * sizeof(double),
                                       cudaMemcpyDeviceToHost, c.stream));
         SIMK_CUDA(cudaStreamSynchronize(c.stream));
+        check_device_error(c);
     });
 }
 

@@ -113,7 +113,10 @@ struct Context {
     long long batch_bytes = 1LL << 30;
     int graphs = 1;
     int col_tile = 0;
+    int tma = 1;            // TMA-pipelined persistent column pass where available
+    int sm_count = 0;
     int64_t launches = 0;
+    DeviceBuffer err_flag;  // int: set by a kernel whose bounded wait ran out
     std::map<std::pair<int, int>, std::unique_ptr<LinePlan>> plans;
     std::map<std::tuple<int, int, double, double, double, double, double, double>, std::unique_ptr<Propagator>> props;
     // workspaces

@@ -28,6 +28,18 @@ void mul_timed(Context& ctx, float2* psi, const float2* f, long long N, int coun
     launch_mul_broadcast(ctx, psi, f, N, count, scale);
 }
 
+// A kernel whose bounded wait ran out set ctx.err_flag: report it (and clear it) after the stream has drained.
+void check_device_error(Context& ctx) {
+    if (!ctx.err_flag.ptr) return;
+    int flag = 0;
+    SIMK_CUDA(cudaMemcpyAsync(&flag, ctx.err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+    if (flag) {
+        SIMK_CUDA(cudaMemsetAsync(ctx.err_flag.ptr, 0, sizeof(int), ctx.stream));
+        throw Error(SIMK_ERR_TIMEOUT, "a device wait for an asynchronous copy ran out; the results are invalid");
+    }
+}
+
 long long batch_size(const Context& ctx, const GridGeom& g, long long count) {
     long long b = ctx.batch;
     if (b <= 0) b = std::max<long long>(1, ctx.batch_bytes / (long long)(g.count() * sizeof(float2)));
@@ -98,6 +110,7 @@ void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, doubl
             propagate_plain(ctx, pot, energy, tx, ty, psi, b, true, copy_out);
     }
     SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+    check_device_error(ctx);
 }
 
 namespace {

@@ -8,6 +8,7 @@
 namespace simk {
 
 long long batch_size(const Context& ctx, const GridGeom& g, long long count);
+void check_device_error(Context& ctx);
 void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, int count, const double* in_re,
                const double* in_im, const std::vector<int>& planes, double* out_re, double* out_im);
 void scan_device(Context& ctx, const simk_probe& probe, const std::vector<PotentialImpl*>& pots, int n_pos,

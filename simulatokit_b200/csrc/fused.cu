@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "engine.cuh"
+#include "tma.cuh"
 
 namespace simk {
 
@@ -351,6 +352,163 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_ct(ColArgs a, const f
     for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
 }
 
+// ---- the persistent TMA-pipelined passes (power-of-two lengths) --------------------------------------------------------
+// Each CTA walks its tiles blockIdx.x, blockIdx.x + gridDim.x, ...: thread 0 starts the asynchronous copies of the
+// next tile (the waves and the matching rows of t or P) into the other shared-memory stage before the CTA transforms
+// the current one, so copies overlap arithmetic and no global load sits inside a transform. The wave part of a stage
+// doubles as the transform's exchange buffer once it has been read. A wait that runs out sets *err, waits (bounded)
+// for the copy it started and makes the whole CTA return.
+
+// Thread 0: wait for stage s, phase (it >> 1) & 1; on timeout record it and drain the other stage's copy.
+__device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool next_issued, int* err, int* abort_flag) {
+    if (!mbar_wait_bounded(&full[s], (uint32_t)((it >> 1) & 1))) {
+        atomicExch(err, 1);
+        *abort_flag = 1;
+        if (next_issued) mbar_wait_bounded(&full[s ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+    }
+}
+
+// columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each.
+template <int N, int TC, int MODE>
+__global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_constant__ CUtensorMap map,
+                                                               const __grid_constant__ CUtensorMap pmap,
+                                                               float2* __restrict__ psi, float pscale, int ny,
+                                                               int count, const float2* __restrict__ tw, int* err) {
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    constexpr int T = N / 8;
+    constexpr int BOXH = N <= 256 ? N : 256;
+    constexpr int NBOX = N / BOXH;
+    constexpr int TILE = N * TC;  // float2 per tile
+    constexpr uint32_t STAGE_BYTES = 2u * TILE * sizeof(float2);
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ int abort_flag;
+    float2* stages = reinterpret_cast<float2*>(smem_tma);
+    const int c = threadIdx.x;
+    const unsigned t = threadIdx.y;
+    const int tid = (int)t * TC + c;
+    const int tiles_per_wave = ny / TC;
+    const long long ntiles = (long long)count * tiles_per_wave;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_barrier_init();
+        abort_flag = 0;
+    }
+    __syncthreads();
+    TwRegs<N> tr;
+    tw_load<N, 1>(tr, t, tw);
+    auto issue = [&](long long tile, int s) {
+        const int b = (int)(tile / tiles_per_wave);
+        const int iy0 = (int)(tile % tiles_per_wave) * TC;
+        float2* dst = stages + s * 2 * TILE;
+        mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+#pragma unroll
+        for (int k = 0; k < NBOX; ++k) {
+            tma_load_2d(dst + k * BOXH * TC, &map, &full[s], 2 * iy0, b * N + k * BOXH);
+            tma_load_2d(dst + TILE + k * BOXH * TC, &pmap, &full[s], 2 * iy0, k * BOXH);
+        }
+    };
+    long long tile = blockIdx.x;
+    if (tid == 0 && tile < ntiles) issue(tile, 0);
+    for (int it = 0; tile < ntiles; tile += gridDim.x, ++it) {
+        const int s = it & 1;
+        float2* buf = stages + s * 2 * TILE;
+        const float2* pbuf = buf + TILE;
+        const long long next = tile + gridDim.x;
+        if (tid == 0) {
+            if (next < ntiles) issue(next, s ^ 1);
+            stage_wait(full, s, it, next < ntiles, err, &abort_flag);
+        }
+        __syncthreads();
+        if (abort_flag) return;
+        float2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = buf[(t + T * i) * TC + c];
+        __syncthreads();  // the wave tile has been read: it becomes the exchange buffer
+        SmemCT<TC> sm{buf + c};
+        const int b = (int)(tile / tiles_per_wave);
+        const int iy = (int)(tile % tiles_per_wave) * TC + c;
+        ct_fft_from<N, 0, -1>(v, t, tr, sm);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], pbuf[(t + T * i) * TC + c]) * pscale;
+        if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, tr, sm);
+        float2* col = psi + (size_t)b * N * ny + iy;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
+        fence_proxy_async_shared();
+        __syncthreads();  // every thread is done with the stage before its next copy
+    }
+}
+
+// rows: tile = RB consecutive rows of one wave (nx % RB == 0); a stage holds those RB rows and the RB rows of t.
+template <int N, int RB>
+__global__ void __launch_bounds__(RB * (N / 8)) fused_rows_tma(float2* __restrict__ psi,
+                                                               const float2* __restrict__ tmul,
+                                                               const float2* __restrict__ tw, int nx, int nrows,
+                                                               int inv, int fwd, float scale, int* err) {
+    extern __shared__ __align__(128) unsigned char smem_rtma[];
+    constexpr int T = N / 8;
+    constexpr int TILE = N * RB;
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ int abort_flag;
+    float2* stages = reinterpret_cast<float2*>(smem_rtma);
+    const unsigned t = threadIdx.x;
+    const int rr = threadIdx.y;
+    const int tid = rr * T + (int)t;
+    const int ntiles = nrows / RB;
+    const bool with_t = (tmul != nullptr);
+    const uint32_t bytes = (uint32_t)(TILE * sizeof(float2));
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_barrier_init();
+        abort_flag = 0;
+    }
+    __syncthreads();
+    TwRegs<N> tr;
+    tw_load<N, 1>(tr, t, tw);
+    auto issue = [&](int tile, int s) {
+        float2* dst = stages + s * 2 * TILE;
+        const int row0 = tile * RB;
+        mbar_arrive_expect_tx(&full[s], with_t ? 2 * bytes : bytes);
+        bulk_load(dst, psi + (size_t)row0 * N, bytes, &full[s]);
+        if (with_t) bulk_load(dst + TILE, tmul + (size_t)(row0 % nx) * N, bytes, &full[s]);
+    };
+    int tile = blockIdx.x;
+    if (tid == 0 && tile < ntiles) issue(tile, 0);
+    for (int it = 0; tile < ntiles; tile += gridDim.x, ++it) {
+        const int s = it & 1;
+        float2* buf = stages + s * 2 * TILE;
+        const float2* tbuf = buf + TILE;
+        const int next = tile + gridDim.x;
+        if (tid == 0) {
+            if (next < ntiles) issue(next, s ^ 1);
+            stage_wait(full, s, it, next < ntiles, err, &abort_flag);
+        }
+        __syncthreads();
+        if (abort_flag) return;
+        float2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = buf[rr * N + t + T * i];
+        __syncthreads();
+        SmemCT<0> sm{buf + rr * N};
+        if (inv) ct_fft_from<N, 0, +1>(v, t, tr, sm);
+        if (with_t) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], tbuf[rr * N + t + T * i]) * scale;
+        } else if (scale != 1.0f) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = v[i] * scale;
+        }
+        if (fwd) ct_fft_from<N, 0, -1>(v, t, tr, sm);
+        float2* row = psi + (size_t)(tile * RB + rr) * N;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
+        fence_proxy_async_shared();
+        __syncthreads();
+    }
+}
+
 // ---- plans and launches ---------------------------------------------------------------------------------------------
 namespace {
 
@@ -477,6 +635,72 @@ void launch_cols_ct_m(Context& ctx, const RegPlan& p, const ColArgs& a, int coun
     ++ctx.launches;
 }
 
+
+
+void ensure_err_flag(Context& ctx) {
+    if (!ctx.err_flag.ptr) {
+        ctx.err_flag.alloc(sizeof(int));
+        SIMK_CUDA(cudaMemsetAsync(ctx.err_flag.ptr, 0, sizeof(int), ctx.stream));
+    }
+    if (ctx.sm_count == 0) SIMK_CUDA(cudaDeviceGetAttribute(&ctx.sm_count, cudaDevAttrMultiProcessorCount, ctx.device));
+}
+
+template <int N>
+bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
+                     int fwd, float scale) {
+    constexpr int T = N / 8;
+    constexpr int RB = (256 / T) > 0 ? (256 / T) : 1;
+    if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
+    const size_t smem = 4 * (size_t)N * RB * sizeof(float2);
+    auto kern = fused_rows_tma<N, RB>;
+    static int blocks_per_sm = -1;
+    if (blocks_per_sm < 0) {
+        SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, RB * T, smem));
+    }
+    if (blocks_per_sm <= 0) return false;
+    ensure_err_flag(ctx);
+    const long long ntiles = nrows / RB;
+    const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
+    kern<<<grid, dim3(T, RB), smem, ctx.stream>>>(psi, tmul, p.tw, nx, (int)nrows, inv, fwd, scale,
+                                                  ctx.err_flag.as<int>());
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+    return true;
+}
+
+template <int N, int TC, int MODE>
+bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    constexpr int T = N / 8;
+    constexpr int BOXH = N <= 256 ? N : 256;
+    const size_t smem = 4 * (size_t)N * TC * sizeof(float2);
+    auto kern = fused_cols_tma<N, TC, MODE>;
+    static int blocks_per_sm = -1;
+    if (blocks_per_sm < 0) {
+        SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, TC * T, smem));
+    }
+    if (blocks_per_sm <= 0) return false;
+    ensure_err_flag(ctx);
+    const CUtensorMap map = encode_tensor_map_2d(a.psi, 2ULL * a.ny, (unsigned long long)count * N, 2 * TC, BOXH);
+    const CUtensorMap pmap = encode_tensor_map_2d(const_cast<float2*>(a.P), 2ULL * a.ny, N, 2 * TC, BOXH);
+    const long long ntiles = (long long)count * (a.ny / TC);
+    const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
+    kern<<<grid, dim3(TC, T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
+                                                  ctx.err_flag.as<int>());
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+    return true;
+}
+
+template <int N, int TC>
+bool launch_cols_tma(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    if (TC < 2 || a.ny % TC) return false;  // the TMA box's inner extent must be a multiple of 16 bytes
+    if (a.mode == 0) return launch_cols_tma_m<N, TC, 0>(ctx, p, a, count);
+    if (a.mode == 1) return launch_cols_tma_m<N, TC, 1>(ctx, p, a, count);
+    return false;
+}
+
 template <int N, int TC>
 void launch_cols_ct(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     switch (a.mode) {
@@ -488,6 +712,17 @@ void launch_cols_ct(Context& ctx, const RegPlan& p, const ColArgs& a, int count)
 
 bool rows_ct(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv, int fwd,
              float scale) {
+    if (ctx.tma) {
+        bool done = false;
+        switch (p.n) {
+            case 256: done = launch_rows_tma<256>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 512: done = launch_rows_tma<512>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 1024: done = launch_rows_tma<1024>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 2048: done = launch_rows_tma<2048>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            default: break;
+        }
+        if (done) return true;
+    }
     switch (p.n) {
         case 128: launch_rows_ct<128>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
         case 256: launch_rows_ct<256>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); return true;
@@ -502,6 +737,14 @@ template <int N>
 bool cols_ct_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
     // TC x N/8 threads per CTA, at most 1024
     if (tc * (N / 8) > 1024 || a.ny % tc) return false;
+    if (ctx.tma && a.mode != 2) {
+        switch (tc) {
+            case 2: if (launch_cols_tma<N, 2>(ctx, p, a, count)) return true; break;
+            case 4: if (launch_cols_tma<N, 4>(ctx, p, a, count)) return true; break;
+            case 8: if constexpr (8 * (N / 8) <= 1024) { if (launch_cols_tma<N, 8>(ctx, p, a, count)) return true; } break;
+            default: break;
+        }
+    }
     switch (tc) {
         case 1: launch_cols_ct<N, 1>(ctx, p, a, count); return true;
         case 2: launch_cols_ct<N, 2>(ctx, p, a, count); return true;
@@ -555,6 +798,32 @@ void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
 }
 
 }  // namespace
+
+
+CUtensorMap encode_tensor_map_2d(void* base, unsigned long long inner, unsigned long long rows, unsigned box_inner,
+                                 unsigned box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SIMK_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        SIMK_REQUIRE(fn != nullptr && q == cudaDriverEntryPointSuccess, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    SIMK_REQUIRE(((uintptr_t)base % 16) == 0, "TMA base address must be 16-byte aligned");
+    SIMK_REQUIRE((inner * sizeof(float)) % 16 == 0, "TMA row pitch must be a multiple of 16 bytes");
+    SIMK_REQUIRE((box_inner * sizeof(float)) % 16 == 0 && box_inner <= 256 && box_rows <= 256, "bad TMA box");
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {inner, rows};
+    const cuuint64_t strides[1] = {inner * sizeof(float)};
+    const cuuint32_t box[2] = {box_inner, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(SIMK_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return map;
+}
 
 bool fused_supported(Context&, const GridGeom& g) { return choose(g.nx).E != 0 && choose(g.ny).E != 0; }
 

@@ -18,12 +18,12 @@ class ExecutionOptions:
     form: "plain" (one operation per launch), "fused" (batched fused passes, the default) or "bf16x3" (fused with
     tensor-core DFT stages). batch: waves per batch (0 = from batch_bytes). batch_bytes: bytes of waves one batch
     may hold (default 1 GiB). graphs: capture each batch's slice loop in a CUDA graph. col_tile: columns per CTA of
-    the fused column pass (0 = automatic)."""
+    the fused column pass (0 = automatic). tma: the TMA-pipelined persistent column pass where available."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
     def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
-                 col_tile: int = 0):
+                 col_tile: int = 0, tma: bool = True):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
         self.form = form
@@ -31,6 +31,7 @@ class ExecutionOptions:
         self.batch_bytes = max(1, int(batch_bytes))
         self.graphs = bool(graphs)
         self.col_tile = int(col_tile)
+        self.tma = bool(tma)
 
     @staticmethod
     def standard() -> "ExecutionOptions":
@@ -73,6 +74,7 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_BATCH_BYTES, o.batch_bytes))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_GRAPHS, 1 if o.graphs else 0))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COL_TILE, o.col_tile))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TMA, 1 if o.tma else 0))
 
     def set_stream(self, stream_ptr: int | None):
         L.check(self.lib.simk_context_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
