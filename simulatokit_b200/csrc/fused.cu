@@ -386,8 +386,8 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
     const int c = threadIdx.x;
     const unsigned t = threadIdx.y;
     const int tid = (int)t * TC + c;
-    const int tiles_per_wave = ny / TC;
-    const long long ntiles = (long long)count * tiles_per_wave;
+    const unsigned tiles_per_wave = (unsigned)(ny / TC);
+    const unsigned ntiles = (unsigned)count * tiles_per_wave;  // < 2^31: checked by the launcher
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -397,9 +397,9 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
     __syncthreads();
     TwRegs<N> tr;
     tw_load<N, 1>(tr, t, tw);
-    auto issue = [&](long long tile, int s) {
+    auto issue = [&](unsigned tile, int s) {
         const int b = (int)(tile / tiles_per_wave);
-        const int iy0 = (int)(tile % tiles_per_wave) * TC;
+        const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
         float2* dst = stages + s * 2 * TILE;
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
 #pragma unroll
@@ -408,13 +408,13 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
             tma_load_2d(dst + TILE + k * BOXH * TC, &pmap, &full[s], 2 * iy0, k * BOXH);
         }
     };
-    long long tile = blockIdx.x;
+    unsigned tile = blockIdx.x;
     if (tid == 0 && tile < ntiles) issue(tile, 0);
     for (int it = 0; tile < ntiles; tile += gridDim.x, ++it) {
         const int s = it & 1;
         float2* buf = stages + s * 2 * TILE;
         const float2* pbuf = buf + TILE;
-        const long long next = tile + gridDim.x;
+        const unsigned next = tile + gridDim.x;
         if (tid == 0) {
             if (next < ntiles) issue(next, s ^ 1);
             stage_wait(full, s, it, next < ntiles, err, &abort_flag);
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
         __syncthreads();  // the wave tile has been read: it becomes the exchange buffer
         SmemCT<TC> sm{buf + c};
         const int b = (int)(tile / tiles_per_wave);
-        const int iy = (int)(tile % tiles_per_wave) * TC + c;
+        const int iy = (int)(tile - (unsigned)b * tiles_per_wave) * TC + c;
         ct_fft_from<N, 0, -1>(v, t, tr, sm);
 #pragma unroll
         for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], pbuf[(t + T * i) * TC + c]) * pscale;
@@ -685,6 +685,7 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     const CUtensorMap map = encode_tensor_map_2d(a.psi, 2ULL * a.ny, (unsigned long long)count * N, 2 * TC, BOXH);
     const CUtensorMap pmap = encode_tensor_map_2d(const_cast<float2*>(a.P), 2ULL * a.ny, N, 2 * TC, BOXH);
     const long long ntiles = (long long)count * (a.ny / TC);
+    if (ntiles >= (1LL << 31)) return false;
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(TC, T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
                                                   ctx.err_flag.as<int>());
