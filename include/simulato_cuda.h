@@ -61,6 +61,12 @@ extern "C" {
 
 typedef struct simk_context simk_context;
 typedef struct simk_potential simk_potential;
+typedef struct simk_surrogate simk_surrogate;
+
+/* Parameters of the finite-projection surrogate network (float32): emb[103][16] | W1[64][18] b1[64] |
+ * W2[64][64] b2[64] | W3[64][64] b3[64] | W4[64] b4[1]. The network is a cumulative profile C(Z, rho, z); a slab's
+ * profile is P_inf(rho) (C(Z, rho, zu) - C(Z, rho, zl)). */
+#define SIMK_SURROGATE_PARAMS 11249
 
 /* Grid (Sources/SimulatoCore/Grid.swift:8-91): nx x ny points over extent_x x extent_y [A]. */
 typedef struct {
@@ -129,6 +135,40 @@ int simk_potential_read_slices(simk_context* ctx, simk_potential* potential, dou
  * Multislice.swift:83-103), as stored on the device (complex64 widened). */
 int simk_potential_read_transmission(simk_context* ctx, simk_potential* potential, double energy, int32_t slice,
                                      double* re, double* im);
+
+/* ---- finite projection and its learned surrogate -------------------------------------------------------------------
+ * No reference implementation: SimulatoKit lists Potential(projection="finite") as not ported (docs/parity.md:58,251).
+ * P(rho; zl, zu) = int_zl^zu V(sqrt(rho^2 + z^2)) dz of the Lobato potential V(r) = sum A_i (2/(B_i r) + 1) e^{-B_i r}
+ * (A, B of LobatoParameterization.swift:38-44), by float64 Gauss-Legendre quadrature on the device, at n points. */
+int simk_finite_profile(simk_context* ctx, int32_t n, const int32_t* atomic_numbers, const double* rho,
+                        const double* zl, const double* zu, double* out);
+/* V of every slice by finite projection (each atom reaches R_c(Z) in the plane and along the beam; xyz wrapped in
+ * x, y). With `surrogate` (may be NULL) the profiles of the pairs inside its trained domain come from the network,
+ * judged on a sample by the quadrature: above `error_bound` (max relative) the quadrature replaces it.
+ * *used_surrogate and *judged_max_rel report what happened. */
+int simk_potential_from_atoms_finite(simk_context* ctx, const simk_grid* grid, int32_t n_slices, const double* thickness,
+                                     int32_t n_atoms, const int32_t* atomic_numbers, const double* xyz,
+                                     simk_surrogate* surrogate, double error_bound, int32_t* used_surrogate,
+                                     double* judged_max_rel, simk_potential** out);
+/* Trains the surrogate on the device: n_samples quadrature-labelled samples of the elements, `steps` Adam steps of
+ * `batch` samples, slabs up to max_thickness A, radii from rho_min A. */
+int simk_surrogate_train(simk_context* ctx, int32_t n_elements, const int32_t* atomic_numbers, int64_t n_samples,
+                         int32_t steps, int32_t batch, double learning_rate, uint64_t seed, double max_thickness,
+                         double rho_min, simk_surrogate** out);
+int simk_surrogate_destroy(simk_surrogate* surrogate);
+/* info[8] = train loss, held-out max and rms error of P in units of P_inf(rho) (|dF|), 0, 1, steps, samples, max
+ * thickness. */
+int simk_surrogate_info(const simk_surrogate* surrogate, double* info);
+int simk_surrogate_evaluate(simk_context* ctx, simk_surrogate* surrogate, int32_t n, const int32_t* atomic_numbers,
+                            const double* rho, const double* zl, const double* zu, double* out);
+/* Reads (get != NULL) and/or replaces (set != NULL) the SIMK_SURROGATE_PARAMS float32 parameters; the target
+ * standardisation (mean, spread) is read into / set from ms[2] when ms != NULL. */
+int simk_surrogate_parameters(simk_context* ctx, simk_surrogate* surrogate, float* get, const float* set, double* ms);
+/* One forward + backward pass on the given batch against targets F = P / P_inf(rho): the loss and the gradient of every
+ * parameter (the training kernels, exposed for gradient checks). */
+int simk_surrogate_gradients(simk_context* ctx, simk_surrogate* surrogate, int32_t n, const int32_t* atomic_numbers,
+                             const double* rho, const double* zl, const double* zu, const double* target,
+                             float* gradients, double* loss);
 
 /* ---- multislice -----------------------------------------------------------------------------------------------------
  * Multislice.run (Multislice.swift:52-80 -> MetalMultislice.run, MetalEngine.swift:458-474): one incident wave through

@@ -783,3 +783,174 @@ def silicon_cell(a0: float = 5.431) -> Structure:
     fcc = np.array([(0, 0, 0), (0, 0.5, 0.5), (0.5, 0, 0.5), (0.5, 0.5, 0)], dtype=np.float64)
     frac = np.concatenate([fcc, fcc + 0.25])
     return Structure((a0, a0, a0), np.full(8, 14), frac * a0)
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# Finite projection (no reference implementation: SimulatoKit lists `Potential(projection="finite")` as not ported,
+# docs/parity.md:58,251). Parity is anchored on identities: the thick-slab limit equals the infinite projection
+# (pins.py:423-446's analytic form), slices add, and the radial profile integrates to the k = 0 value.
+# ---------------------------------------------------------------------------------------------------------------------
+
+def lobato_potential_3d(z: int, r):
+    """V(r) = sum_i A_i (2 / (B_i r) + 1) exp(-B_i r), the real-space Lobato potential whose projection is the
+    infinite projection of LobatoParameterization.swift:51-69 (its 2-D transform is f(k^2))."""
+    A, B = scaled_parameters(z)
+    r = np.asarray(r, dtype=np.float64)
+    return sum(A[i] * (2.0 / (B[i] * r) + 1.0) * np.exp(-B[i] * r) for i in range(5))
+
+
+def infinite_profile(z: int, rho):
+    """Analytic infinite projection 2 sum_i [2 A_i / B_i K0(B_i rho) + A_i rho K1(B_i rho)] (pins.py:432)."""
+    from scipy.special import kn
+    A, B = scaled_parameters(z)
+    rho = np.asarray(rho, dtype=np.float64)
+    return 2 * sum(2 * A[i] / B[i] * kn(0, rho * B[i]) + A[i] * rho * kn(1, rho * B[i]) for i in range(5))
+
+
+def finite_profile(z: int, rho: float, zl: float, zu: float, n: int = 48) -> float:
+    """int_{zl}^{zu} V(sqrt(rho^2 + z^2)) dz with z = rho sinh(u): the integrand sum_i A_i (2/B_i + rho cosh u)
+    exp(-B_i rho cosh u) is smooth in u; n-point Gauss-Legendre on each side of u = 0."""
+    if zu <= zl:
+        return 0.0
+    A, B = scaled_parameters(z)
+    x, w = np.polynomial.legendre.leggauss(n)
+    ul, uu = math.asinh(zl / rho), math.asinh(zu / rho)
+    parts = [(ul, 0.0), (0.0, uu)] if ul < 0.0 < uu else [(ul, uu)]
+    total = 0.0
+    for a, b in parts:
+        u = 0.5 * (b - a) * x + 0.5 * (b + a)
+        c = np.cosh(u)
+        f = sum(A[i] * (2.0 / B[i] + rho * c) * np.exp(-B[i] * rho * c) for i in range(5))
+        total += 0.5 * (b - a) * float(np.dot(w, f))
+    return total
+
+
+def finite_profile_quad(z: int, rho: float, zl: float, zu: float) -> float:
+    """The same integral by adaptive quadrature in z (the independent judge)."""
+    from scipy import integrate
+    f = lambda t: float(lobato_potential_3d(z, math.sqrt(rho * rho + t * t)))  # noqa: E731
+    pts = [0.0] if zl < 0.0 < zu else None
+    return integrate.quad(f, zl, zu, epsabs=0.0, epsrel=1e-13, limit=400, points=pts)[0]
+
+
+def finite_cutoff(z: int, tol: float = 1e-3) -> float:
+    """The radius where V(r) falls to `tol` [V], bounded to [1, 6] A (the truncation of an atom's potential)."""
+    lo, hi = 0.05, 6.0
+    if lobato_potential_3d(z, hi) > tol:
+        return hi
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        if lobato_potential_3d(z, mid) > tol:
+            lo = mid
+        else:
+            hi = mid
+    return max(1.0, hi)
+
+
+def finite_potential_slices(numbers, positions, box, nx, ny, thicknesses, n_gl: int = 48):
+    """Real-space finite-projection potential of every slice: for each atom and slice, the integral of V over the
+    part of the slice within z_a +- R_c, at every pixel within R_c of the atom (periodic in x, y; not in z), with
+    rho clamped below to min(dx, dy) / 2. Small cases only (pure Python loops)."""
+    dx, dy = box[0] / nx, box[1] / ny
+    rmin = 0.5 * min(dx, dy)
+    edges = np.concatenate([[0.0], np.cumsum(thicknesses)])
+    out = np.zeros((len(thicknesses), nx, ny))
+    xs = np.arange(nx) * dx
+    ys = np.arange(ny) * dy
+    for zn, (px, py, pz) in zip(numbers, positions):
+        rc = finite_cutoff(int(zn))
+        ddx = (xs - px + box[0] / 2) % box[0] - box[0] / 2
+        ddy = (ys - py + box[1] / 2) % box[1] - box[1] / 2
+        rho = np.sqrt(ddx[:, None] ** 2 + ddy[None, :] ** 2)
+        mask = rho <= rc
+        for j in range(len(thicknesses)):
+            zl = max(edges[j] - pz, -rc)
+            zu = min(edges[j + 1] - pz, rc)
+            if zu <= zl:
+                continue
+            vals = np.zeros_like(rho)
+            for idx in zip(*np.nonzero(mask)):
+                vals[idx] = finite_profile(int(zn), max(rho[idx], rmin), zl, zu, n_gl)
+            out[j] += vals
+    return out
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# The surrogate network's float64 restatement (checks the device's forward and backward passes)
+# ---------------------------------------------------------------------------------------------------------------------
+
+def surrogate_features(rho, z):
+    """((log rho + 1.5) / 2, asinh(z / rho) / 4): the radius and one slab edge in the u variable of finite_profile,
+    scaled to order one."""
+    rho = np.asarray(rho, dtype=np.float64)
+    return np.stack([(np.log(rho) + 1.5) / 2.0, np.arcsinh(np.asarray(z) / rho) / 4.0], axis=-1)
+
+
+def _silu(x):
+    return x / (1.0 + np.exp(-x))
+
+
+def _silu_grad(x):
+    s = 1.0 / (1.0 + np.exp(-x))
+    return s * (1.0 + x * (1.0 - s))
+
+
+def surrogate_C(params: dict, elem_index, feats):
+    """The cumulative profile network: [emb(Z) (16), 2 features] -> 64 -> 64 -> 64 -> 1, SiLU."""
+    x0 = np.concatenate([params["emb"][elem_index], feats], axis=1)
+    a1 = x0 @ params["W1"].T + params["b1"]
+    h1 = _silu(a1)
+    a2 = h1 @ params["W2"].T + params["b2"]
+    h2 = _silu(a2)
+    a3 = h2 @ params["W3"].T + params["b3"]
+    h3 = _silu(a3)
+    y = h3 @ params["W4"].T + params["b4"]
+    return y[:, 0], (x0, a1, h1, a2, h2, a3, h3)
+
+
+def _surrogate_backward(params, elem_index, cache, dy):
+    x0, a1, h1, a2, h2, a3, h3 = cache
+    dy = dy[:, None]
+    g = {"W4": dy.T @ h3, "b4": dy.sum(0)}
+    d3 = (dy @ params["W4"]) * _silu_grad(a3)
+    g["W3"], g["b3"] = d3.T @ h2, d3.sum(0)
+    d2 = (d3 @ params["W3"]) * _silu_grad(a2)
+    g["W2"], g["b2"] = d2.T @ h1, d2.sum(0)
+    d1 = (d2 @ params["W2"]) * _silu_grad(a1)
+    g["W1"], g["b1"] = d1.T @ x0, d1.sum(0)
+    dx0 = d1 @ params["W1"]
+    emb = np.zeros_like(params["emb"])
+    np.add.at(emb, elem_index, dx0[:, :params["emb"].shape[1]])
+    g["emb"] = emb
+    return g
+
+
+def surrogate_gradients(params: dict, elem_index, rho, zl, zu, fraction):
+    """F_hat = C(rho, zu) - C(rho, zl); mean-squared error against `fraction`; gradients of every parameter."""
+    cu, cache_u = surrogate_C(params, elem_index, surrogate_features(rho, zu))
+    cl, cache_l = surrogate_C(params, elem_index, surrogate_features(rho, zl))
+    e = (cu - cl) - np.asarray(fraction)
+    n = len(e)
+    gu = _surrogate_backward(params, elem_index, cache_u, (2.0 / n) * e)
+    gl = _surrogate_backward(params, elem_index, cache_l, -(2.0 / n) * e)
+    return float(np.mean(e ** 2)), {k: gu[k] + gl[k] for k in gu}
+
+
+def surrogate_unpack(flat) -> dict:
+    """The device's parameter layout: emb[103][16] | W1[64][18] b1 | W2[64][64] b2 | W3[64][64] b3 | W4[64] b4."""
+    f = np.asarray(flat, dtype=np.float64)
+    o = 0
+    out = {}
+    for name, shape in (("emb", (103, 16)), ("W1", (64, 18)), ("b1", (64,)), ("W2", (64, 64)), ("b2", (64,)),
+                        ("W3", (64, 64)), ("b3", (64,)), ("W4", (1, 64)), ("b4", (1,))):
+        n = int(np.prod(shape))
+        out[name] = f[o:o + n].reshape(shape)
+        o += n
+    assert o == f.size
+    return out
+
+
+def surrogate_pack(d: dict) -> np.ndarray:
+    return np.concatenate([np.asarray(d[k], dtype=np.float64).ravel()
+                           for k in ("emb", "W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4")])
+

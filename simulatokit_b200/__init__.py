@@ -11,5 +11,5 @@ from .detector import (STEM, AnnularDetector, CenterOfMassDetector, PixelatedDet
                        SegmentedDetector, detector_shape)
 from .engine import Engine, ExecutionOptions  # noqa: F401
 from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, LobatoParameterization,  # noqa: F401
-                         Multislice, Potential, ProjectedPotential, Slicing)
+                         Multislice, Potential, ProjectedPotential, Slicing, Surrogate, finite_profile)
 from .probe import Aberrations, Aperture, GridScan, Probe  # noqa: F401

@@ -29,8 +29,11 @@ EXPORTED = [
     "simk_context_launch_count", "simk_context_kernel_time", "simk_potential_from_atoms", "simk_potential_from_values", "simk_potential_destroy",
     "simk_potential_slice_count", "simk_potential_read_slices", "simk_potential_read_transmission", "simk_run",
     "simk_run_batch", "simk_probe_spectrum", "simk_build_probes", "simk_detector_shape", "simk_scan",
-    "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc",
+    "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc", "simk_finite_profile",
+    "simk_potential_from_atoms_finite", "simk_surrogate_train", "simk_surrogate_destroy", "simk_surrogate_info",
+    "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients",
 ]
+SURROGATE_PARAMS = 11249
 
 
 class SimulatoError(Exception):
@@ -104,6 +107,15 @@ def _signatures(lib):
                              C.POINTER(P)],
         "simk_fft2": [P, i32, i32, i32, i32, i32, PD, PD, PD, PD],
         "simk_probe_spectrum_noalloc": [C.POINTER(Grid_t), C.POINTER(Probe_t), P, P],
+        "simk_finite_profile": [P, i32, PI32, PD, PD, PD, PD],
+        "simk_potential_from_atoms_finite": [P, C.POINTER(Grid_t), i32, PD, i32, PI32, PD, P, d, PI32, PD,
+                                             C.POINTER(P)],
+        "simk_surrogate_train": [P, i32, PI32, i64, i32, i32, d, C.c_uint64, d, d, C.POINTER(P)],
+        "simk_surrogate_destroy": [P],
+        "simk_surrogate_info": [P, PD],
+        "simk_surrogate_evaluate": [P, P, i32, PI32, PD, PD, PD, PD],
+        "simk_surrogate_parameters": [P, P, C.POINTER(C.c_float), C.POINTER(C.c_float), PD],
+        "simk_surrogate_gradients": [P, P, i32, PI32, PD, PD, PD, PD, C.POINTER(C.c_float), PD],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

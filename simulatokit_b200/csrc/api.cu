@@ -5,8 +5,13 @@
 
 #include "context.cuh"
 #include "engine.cuh"
+#include "surrogate.cuh"
 
 using namespace simk;
+
+struct simk_surrogate {
+    std::unique_ptr<simk::SurrogateImpl> impl;
+};
 
 namespace simk {
 void probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void* out_device, void* stream);
@@ -86,6 +91,7 @@ int simk_context_create(int32_t device, simk_context** out) {
         if (p.major < 10) throw Error(SIMK_ERR_UNAVAILABLE, "the library is built for sm_100a (B200)");
         auto* c = new simk_context();
         c->impl.device = device;
+        c->impl.sm_count = p.multiProcessorCount;
         try {
             SIMK_CUDA(cudaSetDevice(device));
             SIMK_CUDA(cudaStreamCreateWithFlags(&c->impl.own_stream, cudaStreamNonBlocking));
@@ -494,6 +500,144 @@ int simk_fft2(simk_context* ctx, int32_t nx, int32_t ny, int32_t count, int32_t 
 
 int simk_probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void* out_device, void* stream) {
     return guarded([&] { probe_spectrum_noalloc(grid, probe, out_device, stream); });
+}
+
+// ---- finite projection and the surrogate ------------------------------------------------------------------------------
+int simk_finite_profile(simk_context* ctx, int32_t n, const int32_t* atomic_numbers, const double* rho,
+                        const double* zl, const double* zu, double* out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && n >= 0, "bad argument");
+        if (n == 0) return;
+        SIMK_REQUIRE(atomic_numbers && rho && zl && zu && out, "null argument");
+        for (int i = 0; i < n; ++i) {
+            SIMK_REQUIRE(atomic_numbers[i] >= 1 && atomic_numbers[i] <= 103, "unsupported element");
+            SIMK_REQUIRE(std::isfinite(rho[i]) && rho[i] > 0 && std::isfinite(zl[i]) && std::isfinite(zu[i]),
+                         "rho must be positive and the limits finite");
+        }
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        std::vector<int> z(atomic_numbers, atomic_numbers + n);
+        std::vector<double> r(rho, rho + n), l(zl, zl + n), u(zu, zu + n);
+        DeviceBuffer d(n * sizeof(double));
+        surrogate_quadrature_points(ctx->impl, z, r, l, u, d.as<double>());
+        SIMK_CUDA(cudaMemcpy(out, d.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int simk_potential_from_atoms_finite(simk_context* ctx, const simk_grid* grid, int32_t n_slices, const double* thickness,
+                                     int32_t n_atoms, const int32_t* atomic_numbers, const double* xyz,
+                                     simk_surrogate* surrogate, double error_bound, int32_t* used_surrogate,
+                                     double* judged_max_rel, simk_potential** out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && out && used_surrogate && judged_max_rel, "null argument");
+        SIMK_REQUIRE(n_atoms >= 0 && (n_atoms == 0 || (atomic_numbers && xyz)), "null atom arrays");
+        SIMK_REQUIRE(std::isfinite(error_bound) && error_bound > 0, "the error bound must be positive");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        auto p = std::make_unique<simk_potential>();
+        p->impl.ctx = &ctx->impl;
+        p->impl.g = geom_of(grid);
+        p->impl.dz = checked_thickness(n_slices, thickness);
+        int used = 0;
+        double judged = 0.0;
+        build_potential_finite(ctx->impl, p->impl, n_atoms, atomic_numbers, xyz,
+                               surrogate ? surrogate->impl.get() : nullptr, error_bound, &used, &judged);
+        *used_surrogate = used;
+        *judged_max_rel = judged;
+        *out = p.release();
+    });
+}
+
+int simk_surrogate_train(simk_context* ctx, int32_t n_elements, const int32_t* atomic_numbers, int64_t n_samples,
+                         int32_t steps, int32_t batch, double learning_rate, uint64_t seed, double max_thickness,
+                         double rho_min, simk_surrogate** out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && out && atomic_numbers && n_elements >= 1, "null argument");
+        SIMK_REQUIRE(std::isfinite(learning_rate) && learning_rate > 0, "bad learning rate");
+        SIMK_REQUIRE(std::isfinite(max_thickness) && max_thickness > 0 && std::isfinite(rho_min) && rho_min > 0,
+                     "bad domain");
+        SIMK_REQUIRE(n_samples <= (1LL << 27), "at most 2^27 training samples");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        std::vector<int> els(atomic_numbers, atomic_numbers + n_elements);
+        auto s = std::make_unique<simk_surrogate>();
+        s->impl = surrogate_train(ctx->impl, els, n_samples, steps, batch, learning_rate, seed, max_thickness, rho_min);
+        *out = s.release();
+    });
+}
+
+int simk_surrogate_destroy(simk_surrogate* surrogate) {
+    return guarded([&] { delete surrogate; });
+}
+
+int simk_surrogate_info(const simk_surrogate* surrogate, double* info) {
+    return guarded([&] {
+        SIMK_REQUIRE(surrogate && info, "null argument");
+        const SurrogateImpl& s = *surrogate->impl;
+        info[0] = s.train_loss;
+        info[1] = s.val_max_rel;
+        info[2] = s.val_rms_rel;
+        info[3] = s.y_mean;
+        info[4] = s.y_std;
+        info[5] = s.steps;
+        info[6] = (double)s.samples;
+        info[7] = s.max_thickness;
+    });
+}
+
+int simk_surrogate_evaluate(simk_context* ctx, simk_surrogate* surrogate, int32_t n, const int32_t* atomic_numbers,
+                            const double* rho, const double* zl, const double* zu, double* out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && surrogate && n >= 0, "bad argument");
+        if (n == 0) return;
+        SIMK_REQUIRE(atomic_numbers && rho && zl && zu && out, "null argument");
+        for (int i = 0; i < n; ++i)
+            SIMK_REQUIRE(atomic_numbers[i] >= 1 && atomic_numbers[i] <= 103 && rho[i] > 0, "bad query");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        std::vector<int> z(atomic_numbers, atomic_numbers + n);
+        std::vector<double> r(rho, rho + n), l(zl, zl + n), u(zu, zu + n);
+        surrogate_evaluate(ctx->impl, *surrogate->impl, z, r, l, u, out);
+    });
+}
+
+int simk_surrogate_parameters(simk_context* ctx, simk_surrogate* surrogate, float* get, const float* set, double* ms) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && surrogate, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        SurrogateImpl& s = *surrogate->impl;
+        if (get) {
+            SIMK_CUDA(cudaMemcpy(get, s.params.ptr, kSurrogateParams * sizeof(float), cudaMemcpyDeviceToHost));
+            if (ms) {
+                ms[0] = s.y_mean;
+                ms[1] = s.y_std;
+            }
+        }
+        if (set) {
+            SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));  // no launch in flight still reads the old values
+            SIMK_CUDA(cudaMemcpy(s.params.ptr, set, kSurrogateParams * sizeof(float), cudaMemcpyHostToDevice));
+            if (ms && !get) {
+                s.y_mean = ms[0];
+                s.y_std = ms[1];
+            }
+            SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+        }
+    });
+}
+
+int simk_surrogate_gradients(simk_context* ctx, simk_surrogate* surrogate, int32_t n, const int32_t* atomic_numbers,
+                             const double* rho, const double* zl, const double* zu, const double* target,
+                             float* gradients, double* loss) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && surrogate && n >= 1 && atomic_numbers && rho && zl && zu && target && gradients && loss,
+                     "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        std::vector<int> z(atomic_numbers, atomic_numbers + n);
+        std::vector<double> r(rho, rho + n), l(zl, zl + n), u(zu, zu + n), t(target, target + n);
+        *loss = surrogate_gradients(ctx->impl, *surrogate->impl, z, r, l, u, t, gradients);
+    });
 }
 
 }  // extern "C"

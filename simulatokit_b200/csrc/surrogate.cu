@@ -1,0 +1,664 @@
+// surrogate.cu -- a small MLP that stands in for the per-(atom, slice) quadrature of the finite-projection potential.
+//
+// The network C(Z, rho, z) is a cumulative profile: with the element's 16-float embedding and the features
+// ((log rho + 1.5) / 2, asinh(z / rho) / 4) -- the radius and one slice edge in the u variable of finite.cu's
+// quadrature -- it returns the share of the infinite projection below z, so that
+//     P(rho; zl, zu) = P_inf(rho) (C(Z, rho, zu) - C(Z, rho, zl)),
+// P_inf the analytic infinite projection. Slices therefore add exactly, and the loss is the absolute error of the
+// fraction F = P / P_inf, i.e. of P in units of the full projection at that radius -- the error that matters for the
+// summed potential. Network: 18 -> 64 -> 64 -> 64 -> 1 with SiLU.
+// Training (on the device, by the kernels below): samples drawn uniformly in log rho, zl and the slab thickness inside
+// the trained domain, labelled by the float64 quadrature itself; each sample runs the network at both edges (rows b and
+// B + b of a doubled batch) and back-propagates +dF and -dF; mean-squared error; Adam. Every reduction runs in a fixed
+// order, so training is deterministic for a seed. Inference: tensor-core tiles of 16 queries per warp (k_sg_infer),
+// f16 weights and activations, float32 accumulation.
+//
+// Parameter layout (float32, kSurrogateParams values): emb[103][16] | W1[64][18] b1[64] | W2[64][64] b2[64] |
+// W3[64][64] b3[64] | W4[64] b4[1].
+#include <algorithm>
+#include <cmath>
+#include <cuda_fp16.h>
+#include <random>
+
+#include "finite.cuh"
+#include "surrogate.cuh"
+
+namespace simk {
+
+namespace {
+constexpr int OFF_EMB = 0;
+constexpr int OFF_W1 = OFF_EMB + 103 * kEmbed;
+constexpr int OFF_B1 = OFF_W1 + kHidden * kIn;
+constexpr int OFF_W2 = OFF_B1 + kHidden;
+constexpr int OFF_B2 = OFF_W2 + kHidden * kHidden;
+constexpr int OFF_W3 = OFF_B2 + kHidden;
+constexpr int OFF_B3 = OFF_W3 + kHidden * kHidden;
+constexpr int OFF_W4 = OFF_B3 + kHidden;
+constexpr int OFF_B4 = OFF_W4 + kHidden;
+static_assert(OFF_B4 + 1 == kSurrogateParams, "parameter layout");
+
+inline int blocks_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 32)); }
+
+__device__ __forceinline__ float silu(float x) { return x / (1.0f + __expf(-x)); }
+__device__ __forceinline__ float silu_grad(float x) {
+    const float s = 1.0f / (1.0f + __expf(-x));
+    return s * (1.0f + x * (1.0f - s));
+}
+}  // namespace
+
+__host__ __device__ inline void surrogate_features(double rho, double z, float* f) {
+    f[0] = (float)((log(rho) + 1.5) / 2.0);
+    f[1] = (float)(asinh(z / rho) / 4.0);
+}
+
+// ---- training kernels (one output element per thread; reductions over the batch in order) ---------------------------
+__global__ void k_sg_x0(const int* __restrict__ z, const float* __restrict__ feats, const float* __restrict__ emb,
+                        int B, float* __restrict__ x0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B * kIn; i += gridDim.x * blockDim.x) {
+        const int b = i / kIn, k = i % kIn;
+        x0[i] = (k < kEmbed) ? emb[(z[b] - 1) * kEmbed + k] : feats[b * 2 + (k - kEmbed)];
+    }
+}
+
+// Y[b][o] = b[o] + sum_i W[o][i] X[b][i]; with act, H = silu(Y) too.
+__global__ void k_sg_linear(const float* __restrict__ X, const float* __restrict__ W, const float* __restrict__ bias,
+                            int B, int in, int out, float* __restrict__ Y, float* __restrict__ H) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B * out; i += gridDim.x * blockDim.x) {
+        const int b = i / out, o = i % out;
+        float s = bias[o];
+        for (int k = 0; k < in; ++k) s += W[o * in + k] * X[b * in + k];
+        Y[i] = s;
+        if (H) H[i] = silu(s);
+    }
+}
+
+// rows b and B + b of y are C at the upper and the lower edge of sample b: F_hat = y[b] - y[B + b]
+__global__ void k_sg_loss(const float* __restrict__ y, const float* __restrict__ target, int B, float* __restrict__ dy,
+                          double* __restrict__ loss_terms) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+        const float e = (y[b] - y[B + b]) - target[b];
+        dy[b] = 2.0f * e / (float)B;
+        dy[B + b] = -2.0f * e / (float)B;
+        loss_terms[b] = (double)e * (double)e;
+    }
+}
+
+// dW[o][i] = sum_b dY[b][o] X[b][i]; db[o] = sum_b dY[b][o]
+__global__ void k_sg_grad_w(const float* __restrict__ dY, const float* __restrict__ X, int B, int in, int out,
+                            float* __restrict__ dW, float* __restrict__ db) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < out * (in + 1); i += gridDim.x * blockDim.x) {
+        const int o = i / (in + 1), k = i % (in + 1);
+        float s = 0.0f;
+        if (k < in) {
+            for (int b = 0; b < B; ++b) s += dY[b * out + o] * X[b * in + k];
+            dW[o * in + k] = s;
+        } else {
+            for (int b = 0; b < B; ++b) s += dY[b * out + o];
+            db[o] = s;
+        }
+    }
+}
+
+// dX[b][k] = sum_o dY[b][o] W[o][k], times silu'(A[b][k]) when A is given
+__global__ void k_sg_grad_x(const float* __restrict__ dY, const float* __restrict__ W, const float* __restrict__ A,
+                            int B, int in, int out, float* __restrict__ dX) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B * in; i += gridDim.x * blockDim.x) {
+        const int b = i / in, k = i % in;
+        float s = 0.0f;
+        for (int o = 0; o < out; ++o) s += dY[b * out + o] * W[o * in + k];
+        dX[i] = A ? s * silu_grad(A[i]) : s;
+    }
+}
+
+// dEmb[z][k] = sum over the batch's samples of element z of dX0[b][k]
+__global__ void k_sg_grad_emb(const float* __restrict__ dX0, const int* __restrict__ z, int B,
+                              float* __restrict__ demb) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 103 * kEmbed; i += gridDim.x * blockDim.x) {
+        const int zz = i / kEmbed + 1, k = i % kEmbed;
+        float s = 0.0f;
+        for (int b = 0; b < B; ++b)
+            if (z[b] == zz) s += dX0[b * kIn + k];
+        demb[i] = s;
+    }
+}
+
+__global__ void k_sg_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// ---- fused inference ---------------------------------------------------------------------------------------------
+// Each warp evaluates 16 queries (Z, rho, zl, zu) at a time as 32 rows of the network -- rows 0-15 the upper edges,
+// rows 16-31 the lower edges -- with mma.sync m16n8k16 (f16 operands, float32 accumulators):
+//     F = C(zu) - C(zl),   P = P_inf(rho) F.
+// Each block stages the float32 matrices once as f16 [out][in] rows in shared memory (which is the col-major B operand
+// itself; row pitches padded by 16 bytes so that the 8 rows one fragment load touches fall into distinct banks);
+// biases and the 64 -> 1 layer stay float32. The accumulators of one layer, after bias and SiLU, are re-packed in
+// registers as the next layer's A fragments (the m16n8 accumulator layout of two neighbouring n-tiles is the m16k16 A
+// layout), so activations never leave the registers. The 64 -> 1 layer is a quad shuffle-reduction, and the upper and
+// lower rows of a query end in the same lane. f16 rather than bf16: the activations and weights are of order one, and
+// the 11-bit significand keeps the rounding of the hidden activations well below the network's fit.
+struct SgQueryPairs {  // queries from a profile table: pair p, radius k
+    const FinitePair* pairs;
+    const int* pair_ids;      // the table rows this launch fills
+    int npairs;
+    const int* elem_z;        // Z of each element index of the potential
+    const double* rmin;
+    const double* rcut;
+    const double* pinf;       // [element][nr]: P_inf at the table's radii
+    int nr;
+};
+
+constexpr int kTcIn = 32;                            // layer-1 inputs padded to two k-steps
+constexpr int kTcLd1 = kTcIn + 8;                    // padded row pitches (f16 elements)
+constexpr int kTcLd = kHidden + 8;
+constexpr int kTcW1 = kHidden * kTcLd1;
+constexpr int kTcW = kHidden * kTcLd;
+constexpr int kTcWarps = 4;
+constexpr int kTcSmem = (kTcW1 + 2 * kTcW) * 2 + (4 * kHidden + 2) * 4 + kTcWarps * 32 * kTcLd1 * 2;
+
+__device__ __forceinline__ void mma_f16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
+    const __half2 v = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// One hidden layer on 32 rows: acc = A (KS k-steps of 16) x W^T + bias, then SiLU into `out` as the next layer's A
+// fragments (4 k-steps of 16). Fragment layouts of m16n8k16 (g = lane / 4, q = lane % 4): A registers hold
+// (row g, k 2q..2q+1), (row g+8, k 2q..), (row g, k 2q+8..), (row g+8, k 2q+8..); B registers (k 2q.., n g) and
+// (k 2q+8.., n g); accumulators (row g, n 2q, 2q+1) and (row g+8, n 2q, 2q+1).
+template <int KS>
+__device__ __forceinline__ void tc_layer(const uint32_t (&a)[2][KS][4], const __half* __restrict__ W, int ldw,
+                                         const float* __restrict__ bias, int lane, uint32_t (&out)[2][4][4]) {
+    const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const int n = nt * 8 + g;
+        const float b0 = bias[nt * 8 + 2 * q], b1 = bias[nt * 8 + 2 * q + 1];
+        float acc[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            acc[mt][0] = b0;
+            acc[mt][1] = b1;
+            acc[mt][2] = b0;
+            acc[mt][3] = b1;
+        }
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            const uint32_t w0 = *reinterpret_cast<const uint32_t*>(W + n * ldw + ks * 16 + 2 * q);
+            const uint32_t w1 = *reinterpret_cast<const uint32_t*>(W + n * ldw + ks * 16 + 8 + 2 * q);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) mma_f16_16816(acc[mt], a[mt][ks], w0, w1);
+        }
+        // n-tile nt holds columns nt*8 .. nt*8+7: the first (nt even) or second half of the next layer's k-step nt/2
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const uint32_t lo = pack_f16(silu(acc[mt][0]), silu(acc[mt][1]));
+            const uint32_t hi = pack_f16(silu(acc[mt][2]), silu(acc[mt][3]));
+            out[mt][nt >> 1][(nt & 1) * 2] = lo;
+            out[mt][nt >> 1][(nt & 1) * 2 + 1] = hi;
+        }
+    }
+}
+
+template <bool FROM_PAIRS>
+__global__ void __launch_bounds__(kTcWarps * 32) k_sg_infer(const float* __restrict__ params, SgQueryPairs q,
+                                                          const int* __restrict__ qz, const double* __restrict__ qrho,
+                                                          const double* __restrict__ qzl,
+                                                          const double* __restrict__ qzu,
+                                                          const double* __restrict__ qpinf, int nq,
+                                                          double* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_sg[];
+    __half* W1 = reinterpret_cast<__half*>(smem_sg);                 // [64][kTcLd1]
+    __half* W2 = W1 + kTcW1;                                         // [64][kTcLd]
+    __half* W3 = W2 + kTcW;                                          // [64][kTcLd]
+    float* bias = reinterpret_cast<float*>(W3 + kTcW);               // b1 b2 b3 [64 each], W4 [64], b4
+    __half* xs = reinterpret_cast<__half*>(bias + 4 * kHidden + 2);  // per warp [32][kTcLd1]
+    for (int i = threadIdx.x; i < kTcW1; i += blockDim.x) {
+        const int n = i / kTcLd1, k = i % kTcLd1;
+        W1[i] = __float2half_rn(k < kIn ? params[OFF_W1 + n * kIn + k] : 0.0f);
+    }
+    for (int i = threadIdx.x; i < kTcW; i += blockDim.x) {
+        const int n = i / kTcLd, k = i % kTcLd;
+        W2[i] = __float2half_rn(k < kHidden ? params[OFF_W2 + n * kHidden + k] : 0.0f);
+        W3[i] = __float2half_rn(k < kHidden ? params[OFF_W3 + n * kHidden + k] : 0.0f);
+    }
+    for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+        bias[i] = params[OFF_B1 + i];
+        bias[kHidden + i] = params[OFF_B2 + i];
+        bias[2 * kHidden + i] = params[OFF_B3 + i];
+        bias[3 * kHidden + i] = params[OFF_W4 + i];
+    }
+    if (threadIdx.x == 0) bias[4 * kHidden] = params[OFF_B4];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, qd = lane & 3;
+    __half* x = xs + warp * 32 * kTcLd1;
+    const float* w4 = bias + 3 * kHidden;
+    const long long total = FROM_PAIRS ? (long long)q.npairs * q.nr : nq;
+    const long long groups = (total + 15) / 16;
+    for (long long grp = (long long)blockIdx.x * kTcWarps + warp; grp < groups;
+         grp += (long long)gridDim.x * kTcWarps) {
+        // lane l < 16 stages the upper-edge row of query grp*16 + l, lane 16 + l the lower-edge row of the same query
+        const long long qi = grp * 16 + (lane & 15);
+        const bool valid = qi < total;
+        int z = 1;
+        double rho = 1.0, zl = 0.0, zu = 1.0, pinf = 0.0;
+        long long dst = 0;
+        if (valid) {
+            if (FROM_PAIRS) {
+                const int p = q.pair_ids[qi / q.nr], k = (int)(qi % q.nr);
+                const FinitePair pr = q.pairs[p];
+                z = q.elem_z[pr.elem];
+                const double r0 = q.rmin[pr.elem], r1 = q.rcut[pr.elem];
+                rho = r0 * pow(r1 / r0, (double)k / (double)(q.nr - 1));
+                zl = pr.zl;
+                zu = pr.zu;
+                pinf = q.pinf[(size_t)pr.elem * q.nr + k];
+                dst = (long long)p * q.nr + k;
+            } else {
+                z = qz[qi];
+                rho = qrho[qi];
+                zl = qzl[qi];
+                zu = qzu[qi];
+                pinf = qpinf[qi];
+                dst = qi;
+            }
+        }
+        {
+            float f[2];
+            surrogate_features(rho, lane < 16 ? zu : zl, f);
+            __half* row = x + lane * kTcLd1;
+            const float* emb = params + OFF_EMB + (z - 1) * kEmbed;
+#pragma unroll
+            for (int k = 0; k < kEmbed; k += 2)
+                *reinterpret_cast<uint32_t*>(row + k) = pack_f16(__ldg(emb + k), __ldg(emb + k + 1));
+            *reinterpret_cast<uint32_t*>(row + kEmbed) = pack_f16(f[0], f[1]);
+#pragma unroll
+            for (int k = kIn; k < kTcIn; k += 2) *reinterpret_cast<uint32_t*>(row + k) = 0u;
+        }
+        __syncwarp();
+        uint32_t a1[2][2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                const __half* r0 = x + (mt * 16 + g) * kTcLd1 + ks * 16 + 2 * qd;
+                const __half* r1 = r0 + 8 * kTcLd1;
+                a1[mt][ks][0] = *reinterpret_cast<const uint32_t*>(r0);
+                a1[mt][ks][1] = *reinterpret_cast<const uint32_t*>(r1);
+                a1[mt][ks][2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
+                a1[mt][ks][3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
+            }
+        __syncwarp();  // the rows are rewritten by the next group
+        uint32_t h1[2][4][4], h2[2][4][4], h3[2][4][4];
+        tc_layer<2>(a1, W1, kTcLd1, bias, lane, h1);
+        tc_layer<4>(h1, W2, kTcLd, bias + kHidden, lane, h2);
+        tc_layer<4>(h2, W3, kTcLd, bias + 2 * kHidden, lane, h3);
+        // 64 -> 1: this lane holds columns ks*16 + 2qd + {0, 1} (+8) of rows g and g + 8 of each m-tile
+        float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const float2 f2 = __half22float2(*reinterpret_cast<const __half2*>(&h3[mt][ks][r]));
+                    const int c = ks * 16 + 2 * qd + ((r & 2) ? 8 : 0);
+                    y[mt][r & 1] += f2.x * w4[c] + f2.y * w4[c + 1];
+                }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 1);
+                y[mt][h] += __shfl_xor_sync(0xffffffffu, y[mt][h], 2);
+            }
+        // m-tile 0 holds the upper edges, m-tile 1 the lower: rows g and g + 8 are queries g and g + 8 (b4 cancels)
+        const float F0 = y[0][0] - y[1][0], F1 = y[0][1] - y[1][1];
+        // lane l < 16 takes query l from the first lane of quad l % 8
+        const float Fa = __shfl_sync(0xffffffffu, F0, (lane & 7) << 2);
+        const float Fb = __shfl_sync(0xffffffffu, F1, (lane & 7) << 2);
+        const float F = (lane & 8) ? Fb : Fa;
+        if (lane < 16 && valid) out[dst] = pinf * (double)F;
+    }
+}
+
+// ---- host --------------------------------------------------------------------------------------------------------
+double infinite_profile(int z, double rho) {
+    const ElementAB e = element_ab(z);
+    double s = 0.0;
+    for (int t = 0; t < 5; ++t)
+        s += 2.0 * e.A[t] / e.B[t] * std::cyl_bessel_k(0.0, e.B[t] * rho) + e.A[t] * rho * std::cyl_bessel_k(1.0, e.B[t] * rho);
+    return 2.0 * s;
+}
+
+namespace {
+
+struct Batch {  // a doubled batch: rows b (upper edge) and B + b (lower edge)
+    DeviceBuffer z, feats, target, x0, a1, h1, a2, h2, a3, h3, y, dy, d3, d2, d1, dx0, loss;
+    void ensure(int B) {
+        const int R = 2 * B;
+        z.ensure(R * sizeof(int));
+        feats.ensure((size_t)R * 2 * sizeof(float));
+        target.ensure(B * sizeof(float));
+        x0.ensure((size_t)R * kIn * sizeof(float));
+        for (DeviceBuffer* b : {&a1, &h1, &a2, &h2, &a3, &h3, &d3, &d2, &d1}) b->ensure((size_t)R * kHidden * sizeof(float));
+        y.ensure(R * sizeof(float));
+        dy.ensure(R * sizeof(float));
+        dx0.ensure((size_t)R * kIn * sizeof(float));
+        loss.ensure(B * sizeof(double));
+    }
+};
+
+// Host rows of one doubled batch from samples [first, first + B).
+void fill_rows(const std::vector<int>& z, const std::vector<double>& rho, const std::vector<double>& zl,
+               const std::vector<double>& zu, size_t first, int B, std::vector<int>& rz, std::vector<float>& rf) {
+    rz.resize(2 * B);
+    rf.resize(4 * (size_t)B);
+    for (int b = 0; b < B; ++b) {
+        const size_t i = first + b;
+        rz[b] = rz[B + b] = z[i];
+        surrogate_features(rho[i], zu[i], rf.data() + 2 * b);
+        surrogate_features(rho[i], zl[i], rf.data() + 2 * (B + b));
+    }
+}
+
+// Forward and backward of one doubled batch already in b: gradients into G, returns the loss when asked.
+double forward_backward(Context& ctx, const float* P, float* G, Batch& b, int B, bool want_loss) {
+    cudaStream_t s = ctx.stream;
+    const int R = 2 * B;
+    const int bl = blocks_for((long long)R * kHidden);
+    k_sg_x0<<<blocks_for((long long)R * kIn), 256, 0, s>>>(b.z.as<int>(), b.feats.as<float>(), P + OFF_EMB, R,
+                                                           b.x0.as<float>());
+    k_sg_linear<<<bl, 256, 0, s>>>(b.x0.as<float>(), P + OFF_W1, P + OFF_B1, R, kIn, kHidden, b.a1.as<float>(),
+                                   b.h1.as<float>());
+    k_sg_linear<<<bl, 256, 0, s>>>(b.h1.as<float>(), P + OFF_W2, P + OFF_B2, R, kHidden, kHidden, b.a2.as<float>(),
+                                   b.h2.as<float>());
+    k_sg_linear<<<bl, 256, 0, s>>>(b.h2.as<float>(), P + OFF_W3, P + OFF_B3, R, kHidden, kHidden, b.a3.as<float>(),
+                                   b.h3.as<float>());
+    k_sg_linear<<<blocks_for(R), 256, 0, s>>>(b.h3.as<float>(), P + OFF_W4, P + OFF_B4, R, kHidden, 1, b.y.as<float>(),
+                                              nullptr);
+    k_sg_loss<<<blocks_for(B), 256, 0, s>>>(b.y.as<float>(), b.target.as<float>(), B, b.dy.as<float>(),
+                                            b.loss.as<double>());
+    k_sg_grad_w<<<blocks_for(kHidden + 1), 256, 0, s>>>(b.dy.as<float>(), b.h3.as<float>(), R, kHidden, 1, G + OFF_W4,
+                                                        G + OFF_B4);
+    k_sg_grad_x<<<bl, 256, 0, s>>>(b.dy.as<float>(), P + OFF_W4, b.a3.as<float>(), R, kHidden, 1, b.d3.as<float>());
+    k_sg_grad_w<<<blocks_for(kHidden * (kHidden + 1)), 256, 0, s>>>(b.d3.as<float>(), b.h2.as<float>(), R, kHidden,
+                                                                    kHidden, G + OFF_W3, G + OFF_B3);
+    k_sg_grad_x<<<bl, 256, 0, s>>>(b.d3.as<float>(), P + OFF_W3, b.a2.as<float>(), R, kHidden, kHidden,
+                                   b.d2.as<float>());
+    k_sg_grad_w<<<blocks_for(kHidden * (kHidden + 1)), 256, 0, s>>>(b.d2.as<float>(), b.h1.as<float>(), R, kHidden,
+                                                                    kHidden, G + OFF_W2, G + OFF_B2);
+    k_sg_grad_x<<<bl, 256, 0, s>>>(b.d2.as<float>(), P + OFF_W2, b.a1.as<float>(), R, kHidden, kHidden,
+                                   b.d1.as<float>());
+    k_sg_grad_w<<<blocks_for(kHidden * (kIn + 1)), 256, 0, s>>>(b.d1.as<float>(), b.x0.as<float>(), R, kIn, kHidden,
+                                                                G + OFF_W1, G + OFF_B1);
+    k_sg_grad_x<<<blocks_for((long long)R * kIn), 256, 0, s>>>(b.d1.as<float>(), P + OFF_W1, nullptr, R, kIn, kHidden,
+                                                               b.dx0.as<float>());
+    k_sg_grad_emb<<<blocks_for(103 * kEmbed), 256, 0, s>>>(b.dx0.as<float>(), b.z.as<int>(), R, G + OFF_EMB);
+    ctx.launches += 15;
+    SIMK_CUDA(cudaGetLastError());
+    if (!want_loss) return 0.0;
+    std::vector<double> terms(B);
+    SIMK_CUDA(cudaMemcpyAsync(terms.data(), b.loss.ptr, B * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SIMK_CUDA(cudaStreamSynchronize(s));
+    double sum = 0.0;
+    for (double t : terms) sum += t;
+    return sum / B;
+}
+
+void set_infer_smem() {
+    static bool set = false;
+    if (!set) {
+        SIMK_CUDA(cudaFuncSetAttribute(k_sg_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+        SIMK_CUDA(cudaFuncSetAttribute(k_sg_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+        set = true;
+    }
+}
+
+// Persistent grid: at most 4 blocks of 128 threads x 128 registers per SM, and no more warps than 16-query groups.
+inline int infer_blocks(const Context& ctx, long long queries) {
+    const long long groups = (queries + 15) / 16;
+    return (int)std::max<long long>(1, std::min<long long>((groups + kTcWarps - 1) / kTcWarps,
+                                                           4LL * ctx.sm_count));
+}
+
+}  // namespace
+
+// Samples of the trained domain: Z from the list, log rho uniform in [rho_min, R_c(Z)], zl uniform in [-R_c, R_c),
+// thickness uniform in (0, min(max_thickness, R_c - zl)].
+void draw_samples(const SurrogateImpl& s, std::mt19937_64& rng, int n, std::vector<int>& z, std::vector<double>& rho,
+                  std::vector<double>& zl, std::vector<double>& zu) {
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    std::uniform_int_distribution<int> E(0, (int)s.elements.size() - 1);
+    z.resize(n);
+    rho.resize(n);
+    zl.resize(n);
+    zu.resize(n);
+    for (int i = 0; i < n; ++i) {
+        const int e = E(rng);
+        const double rc = s.rcut[e];
+        z[i] = s.elements[e];
+        rho[i] = s.rho_min * std::pow(rc / s.rho_min, U(rng));
+        zl[i] = -rc + 2.0 * rc * U(rng);
+        const double tmax = std::min(s.max_thickness, rc - zl[i]);
+        zu[i] = zl[i] + std::max(1e-4, tmax * U(rng));
+    }
+}
+
+void surrogate_quadrature_points(Context& ctx, const std::vector<int>& z, const std::vector<double>& rho,
+                                 const std::vector<double>& zl, const std::vector<double>& zu, double* out_dev) {
+    const int n = (int)z.size();
+    std::vector<int> els(z);
+    std::sort(els.begin(), els.end());
+    els.erase(std::unique(els.begin(), els.end()), els.end());
+    std::vector<ElementAB> ab;
+    for (int zz : els) ab.push_back(element_ab(zz));
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = (int)(std::lower_bound(els.begin(), els.end(), z[i]) - els.begin());
+    DeviceBuffer dab(ab.size() * sizeof(ElementAB)), didx(n * sizeof(int)), dr(n * sizeof(double)),
+        dl(n * sizeof(double)), du(n * sizeof(double));
+    SIMK_CUDA(cudaMemcpy(dab.ptr, ab.data(), ab.size() * sizeof(ElementAB), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(didx.ptr, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(dr.ptr, rho.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(dl.ptr, zl.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(du.ptr, zu.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    finite_points(ctx, dab.as<ElementAB>(), n, didx.as<int>(), dr.as<double>(), dl.as<double>(), du.as<double>(),
+                  out_dev);
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+std::unique_ptr<SurrogateImpl> surrogate_train(Context& ctx, const std::vector<int>& elements, long long n_samples,
+                                               int steps, int batch, double lr, unsigned long long seed,
+                                               double max_thickness, double rho_min) {
+    SIMK_REQUIRE(!elements.empty(), "no element to train on");
+    SIMK_REQUIRE(n_samples >= batch && batch >= 1 && steps >= 1, "need n_samples >= batch >= 1 and steps >= 1");
+    auto s = std::make_unique<SurrogateImpl>();
+    s->elements = elements;
+    std::sort(s->elements.begin(), s->elements.end());
+    s->elements.erase(std::unique(s->elements.begin(), s->elements.end()), s->elements.end());
+    for (int z : s->elements) {
+        SIMK_REQUIRE(z >= 1 && z <= 103, "unsupported element");
+        s->rcut.push_back(finite_cutoff(z));
+    }
+    s->max_thickness = max_thickness;
+    s->rho_min = rho_min;
+    s->params.alloc(kSurrogateParams * sizeof(float));
+    s->grads.alloc(kSurrogateParams * sizeof(float));
+    s->m.alloc(kSurrogateParams * sizeof(float));
+    s->v.alloc(kSurrogateParams * sizeof(float));
+    // initial weights: U(-1/sqrt(fan_in), 1/sqrt(fan_in)), biases zero, embedding N(0, 0.1)
+    std::mt19937_64 rng(seed);
+    std::vector<float> p(kSurrogateParams, 0.0f);
+    std::normal_distribution<float> N01(0.0f, 0.1f);
+    for (int i = OFF_EMB; i < OFF_W1; ++i) p[i] = N01(rng);
+    auto fill = [&](int off, int count, int fan_in) {
+        std::uniform_real_distribution<float> U(-1.0f / std::sqrt((float)fan_in), 1.0f / std::sqrt((float)fan_in));
+        for (int i = 0; i < count; ++i) p[off + i] = U(rng);
+    };
+    fill(OFF_W1, kHidden * kIn, kIn);
+    fill(OFF_W2, kHidden * kHidden, kHidden);
+    fill(OFF_W3, kHidden * kHidden, kHidden);
+    fill(OFF_W4, kHidden, kHidden);
+    SIMK_CUDA(cudaMemcpy(s->params.ptr, p.data(), kSurrogateParams * sizeof(float), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemset(s->m.ptr, 0, kSurrogateParams * sizeof(float)));
+    SIMK_CUDA(cudaMemset(s->v.ptr, 0, kSurrogateParams * sizeof(float)));
+    // the training set, labelled F = P / P_inf with P by the float64 device quadrature
+    const long long n = n_samples;
+    std::vector<int> all_z(n);
+    std::vector<double> all_rho(n), all_zl(n), all_zu(n);
+    std::vector<float> all_F(n);
+    {
+        DeviceBuffer P(std::min<long long>(n, 1 << 20) * sizeof(double));
+        std::vector<int> z;
+        std::vector<double> rho, zl, zu;
+        for (long long first = 0; first < n; first += (1 << 20)) {
+            const int m = (int)std::min<long long>(1 << 20, n - first);
+            draw_samples(*s, rng, m, z, rho, zl, zu);
+            surrogate_quadrature_points(ctx, z, rho, zl, zu, P.as<double>());
+            std::vector<double> hp(m);
+            SIMK_CUDA(cudaMemcpy(hp.data(), P.ptr, m * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < m; ++i) {
+                all_z[first + i] = z[i];
+                all_rho[first + i] = rho[i];
+                all_zl[first + i] = zl[i];
+                all_zu[first + i] = zu[i];
+                all_F[first + i] = (float)(hp[i] / infinite_profile(z[i], rho[i]));
+            }
+        }
+    }
+    // device copies of the doubled rows of every batch
+    const long long nb = n / batch;
+    DeviceBuffer rows_z((size_t)nb * 2 * batch * sizeof(int)), rows_f((size_t)nb * 4 * batch * sizeof(float));
+    {
+        std::vector<int> rz;
+        std::vector<float> rf;
+        for (long long k = 0; k < nb; ++k) {
+            fill_rows(all_z, all_rho, all_zl, all_zu, (size_t)k * batch, batch, rz, rf);
+            SIMK_CUDA(cudaMemcpy(rows_z.as<int>() + k * 2 * batch, rz.data(), rz.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice));
+            SIMK_CUDA(cudaMemcpy(rows_f.as<float>() + k * 4 * batch, rf.data(), rf.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice));
+        }
+    }
+    DeviceBuffer targets((size_t)n * sizeof(float));
+    SIMK_CUDA(cudaMemcpy(targets.ptr, all_F.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    Batch b;
+    b.ensure(batch);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    double loss = 0.0;
+    for (int step = 0; step < steps; ++step) {
+        const long long k = step % nb;
+        SIMK_CUDA(cudaMemcpyAsync(b.z.ptr, rows_z.as<int>() + k * 2 * batch, 2 * batch * sizeof(int),
+                                  cudaMemcpyDeviceToDevice, ctx.stream));
+        SIMK_CUDA(cudaMemcpyAsync(b.feats.ptr, rows_f.as<float>() + k * 4 * batch, 4 * batch * sizeof(float),
+                                  cudaMemcpyDeviceToDevice, ctx.stream));
+        SIMK_CUDA(cudaMemcpyAsync(b.target.ptr, targets.as<float>() + k * batch, batch * sizeof(float),
+                                  cudaMemcpyDeviceToDevice, ctx.stream));
+        const bool want = (step == steps - 1);
+        const double l = forward_backward(ctx, s->params.as<float>(), s->grads.as<float>(), b, batch, want);
+        if (want) loss = l;
+        // cosine decay from lr to lr / 20
+        const double lr_t = lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(M_PI * step / (double)steps)));
+        const float c1 = 1.0f - std::pow(b1, (float)(step + 1)), c2 = 1.0f - std::pow(b2, (float)(step + 1));
+        k_sg_adam<<<blocks_for(kSurrogateParams), 256, 0, ctx.stream>>>(s->params.as<float>(), s->grads.as<float>(),
+                                                                         s->m.as<float>(), s->v.as<float>(),
+                                                                         kSurrogateParams, (float)lr_t, b1, b2, eps,
+                                                                         c1, c2);
+        ++ctx.launches;
+    }
+    SIMK_CUDA(cudaGetLastError());
+    s->train_loss = loss;
+    s->steps = steps;
+    s->samples = n;
+    // held-out judgement by the quadrature: 4096 fresh samples, error |dP| / P_inf(rho) = |dF|
+    std::vector<int> z;
+    std::vector<double> rho, zl, zu;
+    draw_samples(*s, rng, 4096, z, rho, zl, zu);
+    std::vector<double> q(4096), e(4096);
+    DeviceBuffer dq(4096 * sizeof(double));
+    surrogate_quadrature_points(ctx, z, rho, zl, zu, dq.as<double>());
+    SIMK_CUDA(cudaMemcpy(q.data(), dq.ptr, 4096 * sizeof(double), cudaMemcpyDeviceToHost));
+    surrogate_evaluate(ctx, *s, z, rho, zl, zu, e.data());
+    double mx = 0.0, rms = 0.0;
+    for (int i = 0; i < 4096; ++i) {
+        const double r = std::fabs(e[i] - q[i]) / infinite_profile(z[i], rho[i]);
+        mx = std::max(mx, r);
+        rms += r * r;
+    }
+    s->val_max_rel = mx;
+    s->val_rms_rel = std::sqrt(rms / 4096.0);
+    return s;
+}
+
+void surrogate_evaluate(Context& ctx, const SurrogateImpl& s, const std::vector<int>& z, const std::vector<double>& rho,
+                        const std::vector<double>& zl, const std::vector<double>& zu, double* out_host) {
+    const int n = (int)z.size();
+    if (n == 0) return;
+    set_infer_smem();
+    std::vector<double> pinf(n);
+    for (int i = 0; i < n; ++i) pinf[i] = infinite_profile(z[i], rho[i]);
+    DeviceBuffer dz(n * sizeof(int)), dr(n * sizeof(double)), dl(n * sizeof(double)), du(n * sizeof(double)),
+        dp(n * sizeof(double)), dout(n * sizeof(double));
+    SIMK_CUDA(cudaMemcpy(dz.ptr, z.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(dr.ptr, rho.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(dl.ptr, zl.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(du.ptr, zu.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(dp.ptr, pinf.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SgQueryPairs q{};
+    k_sg_infer<false><<<infer_blocks(ctx, n), kTcWarps * 32, kTcSmem, ctx.stream>>>(
+        s.params.as<float>(), q, dz.as<int>(), dr.as<double>(), dl.as<double>(), du.as<double>(),
+        dp.as<double>(), n, dout.as<double>());
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+    SIMK_CUDA(cudaMemcpyAsync(out_host, dout.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void surrogate_profiles(Context& ctx, const SurrogateImpl& s, const FiniteDevice& d, const int* pair_ids_dev,
+                        int npairs, const int* elem_z_dev, const double* pinf_dev, int nr, double* table) {
+    if (npairs == 0) return;
+    set_infer_smem();
+    SgQueryPairs q{d.pairs, pair_ids_dev, npairs, elem_z_dev, d.rmin, d.rcut, pinf_dev, nr};
+    KernelTimer t(ctx, "surrogate_infer", 0.0);
+    k_sg_infer<true><<<infer_blocks(ctx, (long long)npairs * nr), kTcWarps * 32, kTcSmem, ctx.stream>>>(
+        s.params.as<float>(), q, nullptr, nullptr, nullptr, nullptr, nullptr, 0, table);
+    SIMK_CUDA(cudaGetLastError());
+    ++ctx.launches;
+}
+
+double surrogate_gradients(Context& ctx, SurrogateImpl& s, const std::vector<int>& z, const std::vector<double>& rho,
+                           const std::vector<double>& zl, const std::vector<double>& zu,
+                           const std::vector<double>& target, float* grads_host) {
+    const int B = (int)z.size();
+    SIMK_REQUIRE(B >= 1, "empty batch");
+    Batch b;
+    b.ensure(B);
+    std::vector<int> rz;
+    std::vector<float> rf, y(B);
+    fill_rows(z, rho, zl, zu, 0, B, rz, rf);
+    for (int i = 0; i < B; ++i) y[i] = (float)target[i];
+    SIMK_CUDA(cudaMemcpy(b.z.ptr, rz.data(), rz.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(b.feats.ptr, rf.data(), rf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    SIMK_CUDA(cudaMemcpy(b.target.ptr, y.data(), B * sizeof(float), cudaMemcpyHostToDevice));
+    const double loss = forward_backward(ctx, s.params.as<float>(), s.grads.as<float>(), b, B, true);
+    SIMK_CUDA(cudaMemcpy(grads_host, s.grads.ptr, kSurrogateParams * sizeof(float), cudaMemcpyDeviceToHost));
+    return loss;
+}
+
+}  // namespace simk

@@ -90,12 +90,87 @@ class Slicing:
         return np.minimum(np.searchsorted(edges, z, side="right"), len(thicknesses) - 1).astype(np.int32)
 
 
+class Surrogate:
+    """The learned finite-projection profile: an MLP trained on the device on samples the float64 quadrature labels
+    (no counterpart in SimulatoKit, whose finite projection is not ported, docs/parity.md:58,251)."""
+
+    def __init__(self, elements, n_samples: int = 1_000_000, steps: int = 6000, batch: int = 4096,
+                 learning_rate: float = 2e-3, seed: int = 1, max_thickness: float = 4.0, rho_min: float = 0.01,
+                 engine: Engine | None = None):
+        self.engine = engine or Engine.require()
+        z = np.ascontiguousarray(sorted(set(int(e) for e in elements)), dtype=np.int32)
+        out = C.c_void_p()
+        L.check(self.engine.lib.simk_surrogate_train(self.engine.handle, len(z), L.iptr(z), int(n_samples),
+                                                     int(steps), int(batch), float(learning_rate), int(seed),
+                                                     float(max_thickness), float(rho_min), C.byref(out)))
+        self.handle = out
+        self.elements = [int(v) for v in z]
+        lib = self.engine.lib
+        self._finalizer = __import__("weakref").finalize(self, lambda: lib.simk_surrogate_destroy(out))
+
+    @property
+    def info(self) -> dict:
+        v = np.zeros(8)
+        L.check(self.engine.lib.simk_surrogate_info(self.handle, L.dptr(v)))
+        keys = ["train_loss", "val_max_rel", "val_rms_rel", "y_mean", "y_std", "steps", "samples", "max_thickness"]
+        return dict(zip(keys, v.tolist()))
+
+    def evaluate(self, z, rho, zl, zu) -> np.ndarray:
+        z = np.ascontiguousarray(np.broadcast_to(z, np.shape(rho)), dtype=np.int32).ravel()
+        r, l, u = (np.ascontiguousarray(np.broadcast_to(a, np.shape(rho)), dtype=np.float64).ravel()
+                   for a in (rho, zl, zu))
+        out = np.empty(len(r))
+        L.check(self.engine.lib.simk_surrogate_evaluate(self.engine.handle, self.handle, len(r), L.iptr(z), L.dptr(r),
+                                                        L.dptr(l), L.dptr(u), L.dptr(out)))
+        return out
+
+    def parameters(self, set_to: np.ndarray | None = None, mean_std=None):
+        """The float32 parameters (and the target's mean and spread); with set_to, replace them."""
+        ms = np.zeros(2)
+        if set_to is not None:
+            arr = np.ascontiguousarray(set_to, dtype=np.float32)
+            ms = np.ascontiguousarray(mean_std, dtype=np.float64) if mean_std is not None else None
+            L.check(self.engine.lib.simk_surrogate_parameters(
+                self.engine.handle, self.handle, None, arr.ctypes.data_as(C.POINTER(C.c_float)),
+                L.dptr(ms) if ms is not None else None))
+            return None
+        out = np.empty(L.SURROGATE_PARAMS, dtype=np.float32)
+        L.check(self.engine.lib.simk_surrogate_parameters(self.engine.handle, self.handle,
+                                                          out.ctypes.data_as(C.POINTER(C.c_float)), None, L.dptr(ms)))
+        return out, (float(ms[0]), float(ms[1]))
+
+    def gradients(self, z, rho, zl, zu, target):
+        z = np.ascontiguousarray(z, dtype=np.int32)
+        r, l, u, t = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, zl, zu, target))
+        g = np.empty(L.SURROGATE_PARAMS, dtype=np.float32)
+        loss = C.c_double(0)
+        L.check(self.engine.lib.simk_surrogate_gradients(self.engine.handle, self.handle, len(z), L.iptr(z), L.dptr(r),
+                                                         L.dptr(l), L.dptr(u), L.dptr(t),
+                                                         g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
+        return float(loss.value), g
+
+
+def finite_profile(z, rho, zl, zu, engine: Engine | None = None) -> np.ndarray:
+    """P(rho; zl, zu) = int_zl^zu V(sqrt(rho^2 + z^2)) dz by the device's float64 quadrature."""
+    e = engine or Engine.require()
+    z = np.ascontiguousarray(np.broadcast_to(z, np.shape(rho)), dtype=np.int32).ravel()
+    r, l, u = (np.ascontiguousarray(np.broadcast_to(a, np.shape(rho)), dtype=np.float64).ravel() for a in (rho, zl, zu))
+    out = np.empty(len(r))
+    L.check(e.lib.simk_finite_profile(e.handle, len(r), L.iptr(z), L.dptr(r), L.dptr(l), L.dptr(u), L.dptr(out)))
+    return out
+
+
 class Potential:
-    """A structure sliced on a grid, built on the device when first used (Potential.swift:12-92)."""
+    """A structure sliced on a grid, built on the device when first used (Potential.swift:12-92).
+
+    projection: "infinite" (the reference's Lobato projection, the default) or "finite" (real-space integration of
+    each atom over the slices it reaches; with `surrogate`, the learned profile where trained, judged against the
+    quadrature with `error_bound`)."""
 
     def __init__(self, structure: AtomicStructure, nx: int = None, ny: int = None, slice_thickness: float = None,
                  slice_thicknesses=None, parameterization: LobatoParameterization | None = None, sampling=None,
-                 maximum_slice_count: int = 1_000_000):
+                 maximum_slice_count: int = 1_000_000, projection: str = "infinite",
+                 surrogate: Surrogate | None = None, error_bound: float = 1e-2):
         if sampling is not None:
             sx, sy = (sampling, sampling) if np.isscalar(sampling) else sampling
             g = Grid.from_sampling(structure.box[0], structure.box[1], sx, sy)
@@ -113,6 +188,13 @@ class Potential:
         self.numbers = structure.numbers.astype(np.int32)
         self.positions = Slicing.wrapped(structure)
         self.slice_of_atom = Slicing.slice_indices(self.positions[:, 2], self.slice_thicknesses)
+        if projection not in ("infinite", "finite"):
+            _refuse(f"unknown projection {projection!r}")
+        self.projection = projection
+        self.surrogate = surrogate
+        self.error_bound = float(error_bound)
+        self.used_surrogate = None
+        self.judged_max_rel = None
         self._handles = {}
 
     @property
@@ -132,9 +214,17 @@ class Potential:
             z = np.ascontiguousarray(self.numbers, dtype=np.int32)
             s = np.ascontiguousarray(self.slice_of_atom, dtype=np.int32)
             g = self.grid.c()
-            L.check(engine.lib.simk_potential_from_atoms(engine.handle, C.byref(g), len(dz), L.dptr(dz),
-                                                         self.parameterization.code, len(z), L.iptr(z), L.dptr(xyz),
-                                                         L.iptr(s), C.byref(out)))
+            if self.projection == "finite":
+                used, judged = C.c_int32(0), C.c_double(0)
+                L.check(engine.lib.simk_potential_from_atoms_finite(
+                    engine.handle, C.byref(g), len(dz), L.dptr(dz), len(z), L.iptr(z), L.dptr(xyz),
+                    self.surrogate.handle if self.surrogate else None, self.error_bound, C.byref(used),
+                    C.byref(judged), C.byref(out)))
+                self.used_surrogate, self.judged_max_rel = bool(used.value), float(judged.value)
+            else:
+                L.check(engine.lib.simk_potential_from_atoms(engine.handle, C.byref(g), len(dz), L.dptr(dz),
+                                                             self.parameterization.code, len(z), L.iptr(z),
+                                                             L.dptr(xyz), L.iptr(s), C.byref(out)))
             h = PotentialHandle(engine, out)
             self._handles[id(engine)] = h
         return h

@@ -1,0 +1,192 @@
+"""Finite projection and its learned surrogate on the device, against the float64 oracle.
+
+- the device's float64 quadrature equals the oracle's (1e-12) and the analytic infinite projection for a thick slab;
+- the device's finite-projection potential equals the oracle's pixel-by-pixel quadrature within the cubic log-radial
+  interpolation error (1e-4 of the slice maximum; 5e-5 relative at a pixel), slices add, and the slab total is the
+  infinite profile;
+- the training kernels' gradients equal the oracle network's float64 gradients (1e-3 relative, float32 sums);
+- the network is a cumulative profile C(Z, rho, z), a slab's profile P_inf(rho) (C(zu) - C(zl)); its errors are
+  measured as |dP| / P_inf(rho), the error in units of the full projection at that radius;
+- a trained surrogate is judged by the quadrature on held-out samples and inside potentials, falls back to the
+  quadrature outside its domain or bound, and builds profiles faster than the quadrature it replaces.
+"""
+
+import math
+import time
+
+import numpy as np
+import pytest
+
+from oracle import simk_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+sk = pytest.importorskip("simulatokit_b200")
+
+
+@pytest.fixture(scope="module")
+def engine():
+    return sk.Engine.require()
+
+
+@pytest.fixture(scope="module")
+def surrogate(engine):
+    return sk.Surrogate([6, 8, 14, 79], n_samples=1 << 18, steps=5000, batch=4096, seed=3, engine=engine)
+
+
+def test_device_quadrature_matches_oracle(engine):
+    rng = np.random.default_rng(1)
+    z = rng.choice([6, 8, 14, 38, 79], 64)
+    rho = np.exp(rng.uniform(np.log(0.01), np.log(5.0), 64))
+    zl = rng.uniform(-4, 3, 64)
+    zu = zl + rng.uniform(0.01, 4, 64)
+    got = sk.finite_profile(z, rho, zl, zu, engine)
+    ref = np.array([O.finite_profile(int(a), b, c, d) for a, b, c, d in zip(z, rho, zl, zu)])
+    assert np.max(np.abs(got - ref) / np.abs(ref)) <= 1e-12
+    slab = sk.finite_profile(np.full(5, 79), np.array([0.02, 0.1, 0.5, 1, 2.0]), -25.0, 25.0, engine)
+    inf = O.infinite_profile(79, np.array([0.02, 0.1, 0.5, 1, 2.0]))
+    assert np.max(np.abs(slab - inf) / inf) <= 1e-9
+
+
+def _finite_potential(numbers, positions, box, n, thicknesses, **kw):
+    s = sk.AtomicStructure(box, numbers, positions)
+    return sk.Potential(s, n, n, slice_thicknesses=thicknesses, projection="finite", **kw)
+
+
+def test_device_finite_potential_matches_oracle(engine):
+    box = (6.0, 6.0, 4.0)
+    numbers = [8, 79, 14]
+    positions = [(1.3, 2.1, 0.7), (3.9, 4.2, 2.2), (0.4, 5.5, 3.4)]
+    ref = O.finite_potential_slices(numbers, positions, box, 48, 48, [1.0] * 4, n_gl=48)
+    pot = _finite_potential(numbers, positions, box, 48, [1.0] * 4)
+    v = pot.build(engine).values
+    for j in range(4):
+        assert np.max(np.abs(v[j] - ref[j])) <= 1e-4 * np.max(np.abs(ref[j])), j
+    # two slices of 1 A add up to one slice of 2 A (the same atoms, the same limits)
+    pot2 = _finite_potential(numbers, positions, box, 48, [2.0, 2.0])
+    v2 = pot2.build(engine).values
+    assert np.max(np.abs(v2[0] - (v[0] + v[1]))) <= 1e-6 * np.max(np.abs(v2[0]))
+
+
+def test_thick_slab_total_is_the_infinite_profile(engine):
+    box = (8.0, 8.0, 12.0)
+    pot = _finite_potential([79], [(4.0, 4.0, 6.0)], box, 64, [1.0] * 12)
+    total = pot.build(engine).values.sum(0)
+    rc = O.finite_cutoff(79)
+    for ix, iy in ((36, 32), (40, 40), (44, 32), (32, 52)):
+        rho = math.hypot(ix * 0.125 - 4.0, iy * 0.125 - 4.0)
+        ref = O.finite_profile(79, rho, -rc, rc)
+        assert abs(total[ix, iy] - ref) <= 5e-5 * ref  # cubic interpolation over 192 log-spaced radii
+
+
+def test_training_gradients_match_oracle(engine, surrogate):
+    flat, _ = surrogate.parameters()
+    params = O.surrogate_unpack(flat)
+    rng = np.random.default_rng(5)
+    n = 96
+    z = rng.choice([6, 8, 14, 79], n)
+    rho = np.exp(rng.uniform(np.log(0.02), np.log(3.0), n))
+    zl = rng.uniform(-3, 2, n)
+    zu = zl + rng.uniform(0.05, 3, n)
+    target = rng.uniform(0, 1, n)
+    loss, g = surrogate.gradients(z, rho, zl, zu, target)
+    # the device rounds the features to float32 before the network
+    r32 = lambda a: a.astype(np.float32).astype(np.float64)  # noqa: E731
+    fu, fl = r32(O.surrogate_features(rho, zu)), r32(O.surrogate_features(rho, zl))
+    cu, cache_u = O.surrogate_C(params, z - 1, fu)
+    cl, cache_l = O.surrogate_C(params, z - 1, fl)
+    e = (cu - cl) - r32(target)
+    ref_loss = float(np.mean(e ** 2))
+    gu = O._surrogate_backward(params, z - 1, cache_u, (2.0 / n) * e)
+    gl = O._surrogate_backward(params, z - 1, cache_l, -(2.0 / n) * e)
+    rg = O.surrogate_pack({k: gu[k] + gl[k] for k in gu})
+    assert abs(loss - ref_loss) <= 1e-4 * max(ref_loss, 1e-3)
+    assert np.max(np.abs(g - rg)) <= 1e-3 * np.max(np.abs(rg))
+
+
+def _f16(a):
+    """Round float64 values to float16 through float32, as the device stages them, and back."""
+    return np.asarray(a, np.float32).astype(np.float16).astype(np.float64)
+
+
+def test_tensor_core_inference_matches_oracle_network(engine, surrogate):
+    """The fused inference (f16 weights and activations on the tensor cores, float32 sums) against the oracle's
+    float64 network with the same f16 weights and inputs: what differs is the f16 rounding of the hidden activations
+    and the float32 sums."""
+    flat, _ = surrogate.parameters()
+    p = O.surrogate_unpack(flat)
+    params = {k: (_f16(v) if k in ("emb", "W1", "W2", "W3") else v) for k, v in p.items()}
+    rng = np.random.default_rng(17)
+    n = 1000  # not a multiple of 16: the last group of queries is ragged
+    z = rng.choice([6, 8, 14, 79], n)
+    rho = np.exp(rng.uniform(np.log(0.02), np.log(4.0), n))
+    zl = rng.uniform(-4, 3, n)
+    zu = zl + rng.uniform(0.01, 4, n)
+    got = surrogate.evaluate(z, rho, zl, zu)
+    pinf = np.array([O.infinite_profile(int(a), b) for a, b in zip(z, rho)])
+    fu, fl = _f16(O.surrogate_features(rho, zu)), _f16(O.surrogate_features(rho, zl))
+    ref = O.surrogate_C(params, z - 1, fu)[0] - O.surrogate_C(params, z - 1, fl)[0]
+    err = np.abs(got / pinf - ref)
+    rms, mx = float(np.sqrt(np.mean(err ** 2))), float(np.max(err))
+    print(f"f16 tensor-core inference vs float64 network: rms {rms:.2e}, max {mx:.2e}")
+    assert rms <= 1e-3 and mx <= 5e-3, (rms, mx)
+
+
+def test_trained_surrogate_is_judged_by_the_quadrature(engine, surrogate):
+    info = surrogate.info  # held-out error of P in units of P_inf(rho), i.e. |dF|
+    assert info["val_rms_rel"] <= 1e-2, info
+    rng = np.random.default_rng(9)
+    z = rng.choice([6, 8, 14, 79], 256)
+    rho = np.exp(rng.uniform(np.log(0.05), np.log(2.5), 256))
+    zl = rng.uniform(-2.5, 1.5, 256)
+    zu = zl + rng.uniform(0.5, 2.0, 256)
+    got = surrogate.evaluate(z, rho, zl, zu)
+    ref = sk.finite_profile(z, rho, zl, zu, engine)
+    pinf = np.array([O.infinite_profile(int(a), b) for a, b in zip(z, rho)])
+    err = np.abs(got - ref) / pinf
+    assert np.sqrt(np.mean(err ** 2)) <= 1e-2
+
+
+def _amorphous(n_atoms, box, seed, zs=(6, 8, 14, 79), ps=(0.7, 0.2, 0.08, 0.02), dmin=1.4):
+    rng = np.random.default_rng(seed)
+    pos = []
+    while len(pos) < n_atoms:
+        p = rng.uniform(0, 1, 3) * np.array(box)
+        if pos:
+            d = np.array(pos) - p
+            d[:, :2] -= np.round(d[:, :2] / np.array(box[:2])) * np.array(box[:2])
+            if np.min(np.sum(d * d, axis=1)) < dmin * dmin:
+                continue
+        pos.append(p)
+    return rng.choice(zs, n_atoms, p=ps), np.array(pos)
+
+
+def test_surrogate_potential_fallback_and_gain(engine, surrogate):
+    box = (16.0, 16.0, 8.0)
+    nums, pos = _amorphous(160, box, 4)
+    q = _finite_potential(nums, pos, box, 128, [1.0] * 8)
+    engine.set_timing(True)
+    engine.kernel_time("finite_quadrature", reset=True)
+    vq = q.build(engine).values
+    tq = engine.kernel_time("finite_quadrature")[0]
+    s = _finite_potential(nums, pos, box, 128, [1.0] * 8, surrogate=surrogate, error_bound=0.05)
+    vs = s.build(engine).values
+    ts = engine.kernel_time("surrogate_infer")[0]
+    engine.set_timing(False)
+    assert s.used_surrogate and s.judged_max_rel <= 0.05
+    rel_l2 = np.linalg.norm(vs - vq) / np.linalg.norm(vq)
+    assert rel_l2 <= 3e-2, rel_l2
+    print(f"profile tables: surrogate {ts * 1e3:.1f} us, quadrature {tq * 1e3:.1f} us, potential rel-l2 {rel_l2:.2e}, "
+          f"judged max {s.judged_max_rel:.2e}")
+    assert ts < tq, (ts, tq)  # what the network gains: the profile tables in less time than the quadrature
+    # a bound the network cannot meet: the quadrature replaces it, exactly
+    t = _finite_potential(nums, pos, box, 128, [1.0] * 8, surrogate=surrogate, error_bound=1e-9)
+    vt = t.build(engine).values
+    assert not t.used_surrogate
+    assert np.array_equal(vt, vq)
+    # an element it was not trained on: those pairs go to the quadrature
+    nums2 = nums.copy()
+    nums2[0] = 13
+    u = _finite_potential(nums2, pos, box, 128, [1.0] * 8, surrogate=surrogate, error_bound=0.05)
+    u.build(engine)
+    assert u.used_surrogate
