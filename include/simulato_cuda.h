@@ -33,7 +33,8 @@ extern "C" {
 /* ---- execution forms (the metric's A/B pair) ---- */
 #define SIMK_FORM_PLAIN 0   /* one operation per launch, FP32 Stockham FFT in shared memory */
 #define SIMK_FORM_FUSED 1   /* batched: transmission/propagator fused into register-resident FFT passes, FP32 */
-#define SIMK_FORM_BF16X3 2  /* FUSED with the radix DFT stages on tensor cores, 3-term split BF16, FP32 accumulate */
+#define SIMK_FORM_BF16X3 2  /* FUSED with radix-16 DFT stages on tensor cores: split BF16 (data hi+lo, DFT matrix
+                               hi+lo+lo2), FP32 accumulate; grid sides 256, 512, 768, 1024, 2048 */
 
 /* ---- context options (the ExecutionOptions analogue, Sources/SimulatoMultislice/ExecutionOptions.swift:21-49) ---- */
 #define SIMK_OPT_FORM 0         /* one of SIMK_FORM_* (default SIMK_FORM_FUSED) */

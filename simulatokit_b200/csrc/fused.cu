@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "engine.cuh"
+#include "tcfft.cuh"
 #include "tma.cuh"
 
 namespace simk {
@@ -369,7 +370,9 @@ __device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool n
 }
 
 // columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each.
-template <int N, int TC, int MODE>
+// ENG 0: register-resident float32 Cooley-Tukey passes; ENG 1: the tile is transformed in place in shared memory with
+// radix-16 tensor-core stages (tcfft.cuh, the bf16x3 form).
+template <int N, int TC, int MODE, int ENG>
 __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_constant__ CUtensorMap map,
                                                                const __grid_constant__ CUtensorMap pmap,
                                                                float2* __restrict__ psi, float pscale, int ny,
@@ -395,8 +398,9 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
         abort_flag = 0;
     }
     __syncthreads();
-    TwRegs<N> tr;
-    tw_load<N, 1>(tr, t, tw);
+    [[maybe_unused]] std::conditional_t<ENG == 0, TwRegs<N>, Dft16Frags> eng;
+    if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
+    else eng = dft16_frags(tid & 31);
     auto issue = [&](unsigned tile, int s) {
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
@@ -421,27 +425,38 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
         }
         __syncthreads();
         if (abort_flag) return;
-        float2 v[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = buf[(t + T * i) * TC + c];
-        __syncthreads();  // the wave tile has been read: it becomes the exchange buffer
-        SmemCT<TC> sm{buf + c};
         const int b = (int)(tile / tiles_per_wave);
         const int iy = (int)(tile - (unsigned)b * tiles_per_wave) * TC + c;
-        ct_fft_from<N, 0, -1>(v, t, tr, sm);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], pbuf[(t + T * i) * TC + c]) * pscale;
-        if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, tr, sm);
         float2* col = psi + (size_t)b * N * ny + iy;
+        if constexpr (ENG == 0) {
+            float2 v[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
+            for (int i = 0; i < 8; ++i) v[i] = buf[(t + T * i) * TC + c];
+            __syncthreads();  // the wave tile has been read: it becomes the exchange buffer
+            SmemCT<TC> sm{buf + c};
+            ct_fft_from<N, 0, -1>(v, t, eng, sm);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], pbuf[(t + T * i) * TC + c]) * pscale;
+            if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, eng, sm);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
+        } else {
+            tc_fft<N, TC, true, -1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid);
+            if constexpr (MODE == 0) tc_fft<N, TC, true, +1, PRE_MUL>(buf, pbuf, pscale, tw, eng, tid);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                float2 v = buf[(t + T * i) * TC + c];
+                if constexpr (MODE == 1) v = cmul(v, pbuf[(t + T * i) * TC + c]) * pscale;
+                col[(size_t)(t + T * i) * ny] = v;
+            }
+        }
         fence_proxy_async_shared();
         __syncthreads();  // every thread is done with the stage before its next copy
     }
 }
 
 // rows: tile = RB consecutive rows of one wave (nx % RB == 0); a stage holds those RB rows and the RB rows of t.
-template <int N, int RB>
+template <int N, int RB, int ENG>
 __global__ void __launch_bounds__(RB * (N / 8)) fused_rows_tma(float2* __restrict__ psi,
                                                                const float2* __restrict__ tmul,
                                                                const float2* __restrict__ tw, int nx, int nrows,
@@ -465,8 +480,9 @@ __global__ void __launch_bounds__(RB * (N / 8)) fused_rows_tma(float2* __restric
         abort_flag = 0;
     }
     __syncthreads();
-    TwRegs<N> tr;
-    tw_load<N, 1>(tr, t, tw);
+    [[maybe_unused]] std::conditional_t<ENG == 0, TwRegs<N>, Dft16Frags> eng;
+    if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
+    else eng = dft16_frags(tid & 31);
     auto issue = [&](int tile, int s) {
         float2* dst = stages + s * 2 * TILE;
         const int row0 = tile * RB;
@@ -487,23 +503,37 @@ __global__ void __launch_bounds__(RB * (N / 8)) fused_rows_tma(float2* __restric
         }
         __syncthreads();
         if (abort_flag) return;
-        float2 v[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = buf[rr * N + t + T * i];
-        __syncthreads();
-        SmemCT<0> sm{buf + rr * N};
-        if (inv) ct_fft_from<N, 0, +1>(v, t, tr, sm);
-        if (with_t) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], tbuf[rr * N + t + T * i]) * scale;
-        } else if (scale != 1.0f) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = v[i] * scale;
-        }
-        if (fwd) ct_fft_from<N, 0, -1>(v, t, tr, sm);
         float2* row = psi + (size_t)(tile * RB + rr) * N;
+        if constexpr (ENG == 0) {
+            float2 v[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
+            for (int i = 0; i < 8; ++i) v[i] = buf[rr * N + t + T * i];
+            __syncthreads();
+            SmemCT<0> sm{buf + rr * N};
+            if (inv) ct_fft_from<N, 0, +1>(v, t, eng, sm);
+            if (with_t) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], tbuf[rr * N + t + T * i]) * scale;
+            } else if (scale != 1.0f) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = v[i] * scale;
+            }
+            if (fwd) ct_fft_from<N, 0, -1>(v, t, eng, sm);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
+        } else {
+            if (inv) tc_fft<N, RB, false, +1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid);
+            if (fwd) {
+                if (with_t) tc_fft<N, RB, false, -1, PRE_MUL>(buf, tbuf, scale, tw, eng, tid);
+                else tc_fft<N, RB, false, -1, PRE_SCALE>(buf, nullptr, scale, tw, eng, tid);
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                float2 v = buf[rr * N + t + T * i];
+                if (!fwd) v = with_t ? cmul(v, tbuf[rr * N + t + T * i]) * scale : v * scale;
+                row[t + T * i] = v;
+            }
+        }
         fence_proxy_async_shared();
         __syncthreads();
     }
@@ -645,14 +675,14 @@ void ensure_err_flag(Context& ctx) {
     if (ctx.sm_count == 0) SIMK_CUDA(cudaDeviceGetAttribute(&ctx.sm_count, cudaDevAttrMultiProcessorCount, ctx.device));
 }
 
-template <int N>
+template <int N, int ENG>
 bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
                      int fwd, float scale) {
     constexpr int T = N / 8;
     constexpr int RB = (256 / T) > 0 ? (256 / T) : 1;
     if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
     const size_t smem = 4 * (size_t)N * RB * sizeof(float2);
-    auto kern = fused_rows_tma<N, RB>;
+    auto kern = fused_rows_tma<N, RB, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -669,12 +699,12 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     return true;
 }
 
-template <int N, int TC, int MODE>
+template <int N, int TC, int MODE, int ENG>
 bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     constexpr int T = N / 8;
     constexpr int BOXH = N <= 256 ? N : 256;
     const size_t smem = 4 * (size_t)N * TC * sizeof(float2);
-    auto kern = fused_cols_tma<N, TC, MODE>;
+    auto kern = fused_cols_tma<N, TC, MODE, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -694,11 +724,11 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     return true;
 }
 
-template <int N, int TC>
+template <int N, int TC, int ENG = 0>
 bool launch_cols_tma(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     if (TC < 2 || a.ny % TC) return false;  // the TMA box's inner extent must be a multiple of 16 bytes
-    if (a.mode == 0) return launch_cols_tma_m<N, TC, 0>(ctx, p, a, count);
-    if (a.mode == 1) return launch_cols_tma_m<N, TC, 1>(ctx, p, a, count);
+    if (a.mode == 0) return launch_cols_tma_m<N, TC, 0, ENG>(ctx, p, a, count);
+    if (a.mode == 1) return launch_cols_tma_m<N, TC, 1, ENG>(ctx, p, a, count);
     return false;
 }
 
@@ -716,10 +746,10 @@ bool rows_ct(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, in
     if (ctx.tma) {
         bool done = false;
         switch (p.n) {
-            case 256: done = launch_rows_tma<256>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
-            case 512: done = launch_rows_tma<512>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
-            case 1024: done = launch_rows_tma<1024>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
-            case 2048: done = launch_rows_tma<2048>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 256: done = launch_rows_tma<256, 0>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 512: done = launch_rows_tma<512, 0>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 1024: done = launch_rows_tma<1024, 0>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
+            case 2048: done = launch_rows_tma<2048, 0>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
             default: break;
         }
         if (done) return true;
@@ -770,9 +800,65 @@ bool cols_ct(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     }
 }
 
+// ---- the bf16x3 form: the same TMA passes with tensor-core line FFTs ---------------------------------------------------
+bool rows_tc(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv, int fwd,
+             float scale) {
+    switch (p.n) {
+        case 256: return launch_rows_tma<256, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 512: return launch_rows_tma<512, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 768: return launch_rows_tma<768, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 1024: return launch_rows_tma<1024, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 2048: return launch_rows_tma<2048, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        default: return false;
+    }
+}
+
+// The widest column tile (at most the context's SIMK_OPT_COL_TILE, default 4) whose two stages fit in shared memory.
+template <int N>
+bool cols_tc_n(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
+    for (; tc >= 2; tc /= 2) {
+        switch (tc) {
+            case 8:
+                if constexpr (8 * (N / 8) <= 1024) {
+                    if (launch_cols_tma<N, 8, 1>(ctx, p, a, count)) return true;
+                }
+                break;
+            case 4:
+                if constexpr (4 * (N / 8) <= 1024) {
+                    if (launch_cols_tma<N, 4, 1>(ctx, p, a, count)) return true;
+                }
+                break;
+            case 2:
+                if (launch_cols_tma<N, 2, 1>(ctx, p, a, count)) return true;
+                break;
+            default: break;
+        }
+    }
+    return false;
+}
+
+bool cols_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    int tc = ctx.col_tile > 0 ? ctx.col_tile : 4;
+    switch (p.n) {
+        case 256: return cols_tc_n<256>(ctx, p, a, count, tc);
+        case 512: return cols_tc_n<512>(ctx, p, a, count, tc);
+        case 768: return cols_tc_n<768>(ctx, p, a, count, tc);
+        case 1024: return cols_tc_n<1024>(ctx, p, a, count, tc);
+        case 2048: return cols_tc_n<2048>(ctx, p, a, count, tc);
+        default: return false;
+    }
+}
+
+bool tc_length(int n) { return n == 256 || n == 512 || n == 768 || n == 1024 || n == 2048; }
+
 void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
                  int fwd, float scale) {
     KernelTimer timer(ctx, "fused_rows", 16.0 * (double)nrows * p.n);
+    if (ctx.form == SIMK_FORM_BF16X3) {
+        if (!rows_tc(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale))
+            throw Error(SIMK_ERR_INVALID, "the bf16x3 form has no row pass for length " + std::to_string(p.n));
+        return;
+    }
     if (rows_ct(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return;
     switch (p.E) {
         case 8: launch_rows_e<8>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
@@ -787,6 +873,11 @@ void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul
 void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     const double bytes = (a.mode == 2 ? 8.0 : 16.0) * (double)p.n * a.ny * count;
     KernelTimer timer(ctx, "fused_cols", bytes);
+    if (ctx.form == SIMK_FORM_BF16X3 && a.mode != 2) {  // the probe's inverse transform (mode 2) stays float32
+        if (!cols_tc(ctx, p, a, count))
+            throw Error(SIMK_ERR_INVALID, "the bf16x3 form has no column pass for length " + std::to_string(p.n));
+        return;
+    }
     if (cols_ct(ctx, p, a, count)) return;
     switch (p.E) {
         case 8: launch_cols_e<8>(ctx, p, a, count); break;
@@ -826,7 +917,15 @@ CUtensorMap encode_tensor_map_2d(void* base, unsigned long long inner, unsigned 
     return map;
 }
 
-bool fused_supported(Context&, const GridGeom& g) { return choose(g.nx).E != 0 && choose(g.ny).E != 0; }
+bool fused_supported(Context& ctx, const GridGeom& g) {
+    if (ctx.form == SIMK_FORM_BF16X3) {
+        SIMK_REQUIRE(tc_length(g.nx) && tc_length(g.ny),
+                     "the bf16x3 form covers grid sides of 256, 512, 768, 1024 and 2048 points");
+        SIMK_REQUIRE(ctx.tma, "the bf16x3 form runs on the TMA-pipelined passes (SIMK_OPT_TMA must be on)");
+        return true;
+    }
+    return choose(g.nx).E != 0 && choose(g.ny).E != 0;
+}
 
 void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
                      bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last) {
