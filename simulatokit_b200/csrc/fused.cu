@@ -372,8 +372,13 @@ __device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool n
 // columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each.
 // ENG 0: register-resident float32 Cooley-Tukey passes; ENG 1: the tile is transformed in place in shared memory with
 // radix-16 tensor-core stages (tcfft.cuh, the bf16x3 form).
+// Blocks per SM the tensor-core engine asks the compiler for: two when a block has at most 256 threads (at most 128
+// registers a thread), else one.
+constexpr int tc_min_blocks(int threads, int eng) { return (eng == 1 && threads <= 256) ? 2 : 1; }
+
 template <int N, int TC, int MODE, int ENG>
-__global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG))
+    fused_cols_tma(const __grid_constant__ CUtensorMap map,
                                                                const __grid_constant__ CUtensorMap pmap,
                                                                float2* __restrict__ psi, float pscale, int ny,
                                                                int count, const float2* __restrict__ tw, int* err) {
@@ -441,12 +446,17 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
 #pragma unroll
             for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
         } else {
-            tc_fft<N, TC, true, -1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid);
-            if constexpr (MODE == 0) tc_fft<N, TC, true, +1, PRE_MUL>(buf, pbuf, pscale, tw, eng, tid);
+            using L = TileLayout<N, TC, true>;
+            float2* scratch = stages + 4 * TILE;
+            float2* out = tc_fft<N, TC, true, -1, PRE_NONE, true>(buf, scratch, nullptr, 1.0f, tw, eng, tid);
+            if constexpr (MODE == 0) {
+                float2* other = (out == buf) ? scratch : buf;
+                out = tc_fft<N, TC, true, +1, PRE_MUL, false>(out, other, pbuf, pscale, tw, eng, tid);
+            }
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                float2 v = buf[(t + T * i) * TC + c];
-                if constexpr (MODE == 1) v = cmul(v, pbuf[(t + T * i) * TC + c]) * pscale;
+                float2 v = out[L::at(c, (int)t + T * i)];
+                if constexpr (MODE == 1) v = cmul(v, pbuf[L::nat(c, (int)t + T * i)]) * pscale;
                 col[(size_t)(t + T * i) * ny] = v;
             }
         }
@@ -457,7 +467,7 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_tma(const __grid_cons
 
 // rows: tile = RB consecutive rows of one wave (nx % RB == 0); a stage holds those RB rows and the RB rows of t.
 template <int N, int RB, int ENG>
-__global__ void __launch_bounds__(RB * (N / 8)) fused_rows_tma(float2* __restrict__ psi,
+__global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)) fused_rows_tma(float2* __restrict__ psi,
                                                                const float2* __restrict__ tmul,
                                                                const float2* __restrict__ tw, int nx, int nrows,
                                                                int inv, int fwd, float scale, int* err) {
@@ -522,16 +532,27 @@ __global__ void __launch_bounds__(RB * (N / 8)) fused_rows_tma(float2* __restric
 #pragma unroll
             for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
         } else {
-            if (inv) tc_fft<N, RB, false, +1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid);
+            using L = TileLayout<N, RB, false>;
+            float2* scratch = stages + 4 * TILE;
+            float2* out = buf;
+            if (inv) out = tc_fft<N, RB, false, +1, PRE_NONE, true>(buf, scratch, nullptr, 1.0f, tw, eng, tid);
             if (fwd) {
-                if (with_t) tc_fft<N, RB, false, -1, PRE_MUL>(buf, tbuf, scale, tw, eng, tid);
-                else tc_fft<N, RB, false, -1, PRE_SCALE>(buf, nullptr, scale, tw, eng, tid);
+                float2* other = (out == buf) ? scratch : buf;
+                if (inv) {
+                    if (with_t) out = tc_fft<N, RB, false, -1, PRE_MUL, false>(out, other, tbuf, scale, tw, eng, tid);
+                    else out = tc_fft<N, RB, false, -1, PRE_SCALE, false>(out, other, nullptr, scale, tw, eng, tid);
+                } else {
+                    if (with_t) out = tc_fft<N, RB, false, -1, PRE_MUL, true>(out, other, tbuf, scale, tw, eng, tid);
+                    else out = tc_fft<N, RB, false, -1, PRE_SCALE, true>(out, other, nullptr, scale, tw, eng, tid);
+                }
             }
+            const bool moved = inv || fwd;  // a transform ran: the tile is in the working layout
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                float2 v = buf[rr * N + t + T * i];
-                if (!fwd) v = with_t ? cmul(v, tbuf[rr * N + t + T * i]) * scale : v * scale;
-                row[t + T * i] = v;
+                const int idx = (int)t + T * i;
+                float2 v = out[moved ? L::at(rr, idx) : L::nat(rr, idx)];
+                if (!fwd) v = with_t ? cmul(v, tbuf[L::nat(rr, idx)]) * scale : v * scale;
+                row[idx] = v;
             }
         }
         fence_proxy_async_shared();
@@ -681,7 +702,8 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     constexpr int T = N / 8;
     constexpr int RB = (256 / T) > 0 ? (256 / T) : 1;
     if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
-    const size_t smem = 4 * (size_t)N * RB * sizeof(float2);
+    // two stages of (rows, t rows), plus the tensor-core engine's scratch tile
+    const size_t smem = (ENG == 1 ? 5 : 4) * (size_t)N * RB * sizeof(float2);
     auto kern = fused_rows_tma<N, RB, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
@@ -703,7 +725,8 @@ template <int N, int TC, int MODE, int ENG>
 bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     constexpr int T = N / 8;
     constexpr int BOXH = N <= 256 ? N : 256;
-    const size_t smem = 4 * (size_t)N * TC * sizeof(float2);
+    // two stages of (wave tile, P tile), plus the tensor-core engine's scratch tile
+    const size_t smem = (ENG == 1 ? 5 : 4) * (size_t)N * TC * sizeof(float2);
     auto kern = fused_cols_tma<N, TC, MODE, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
