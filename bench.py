@@ -12,6 +12,10 @@ synchronised and barriered on both sides, max over ranks. The waves of a batch (
 no flush is needed between steps. `e2e`: the public `STEM.scan` call from host arrays (structure -> potential built on
 the device -> scan -> detector images back to the host), wall-clocked per call.
 
+`forms`: after the headline, one timed scan of each form (plain float32, fused float32, bf16x3 split-BF16 tensor-core
+stages) on the same stream, and, with the CPU leg, each form's relative L2 error per detector image against the float64
+oracle at the CPU leg's sample positions (the bound for every form is 1e-4).
+
 `--impl reference`: the reference's CPU path (restated in float64 NumPy, oracle/simk_oracle.py; the Swift original
 cannot build on Linux) timed on the host cores on a bounded sample of positions of the same workload.
 """
@@ -136,9 +140,15 @@ def traffic_from_profiles(kernel: str):
 # CPU: the reference's path restated (oracle), on host threads over positions
 # ---------------------------------------------------------------------------------------------------------------------
 
-def cpu_reference(n_positions: int, threads: int):
+def sample_indices(n_positions: int):
+    """The positions of the scan the CPU legs run: every (4096 / n)-th position."""
+    return np.arange(SCAN_N * SCAN_N)[:: max(1, (SCAN_N * SCAN_N) // n_positions)][:n_positions]
+
+
+def cpu_reference(n_positions: int, threads: int, want_values: bool = False):
     """Times the float64 CPU restatement of STEM.cpuScan on `n_positions` positions of the workload (transmissions
-    computed once, as runBatch shares them), `threads` positions at a time. Returns (steps/s, seconds, positions)."""
+    computed once, as runBatch shares them), `threads` positions at a time. Returns (steps/s, seconds, positions) and,
+    with want_values, the detector values at those positions ([detector][position])."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import simk_oracle as O
     box, nums, pos = srtio3(8, 8, 20)
@@ -148,7 +158,7 @@ def cpu_reference(n_positions: int, threads: int):
     ts = [O.transmission(v, ENERGY, g) for v in p.build()]
     spec = O.ProbeSpec(ENERGY, SEMIANGLE)
     dets = [O.DetectorSpec("annular", {"inner": a, "outer": b}) for _, a, b in DETECTORS]
-    positions = scan_positions()[:: max(1, (SCAN_N * SCAN_N) // n_positions)][:n_positions]
+    positions = scan_positions()[sample_indices(n_positions)]
 
     def one(q):
         psi0 = O.build_probe(spec, g, positions[q])
@@ -159,9 +169,12 @@ def cpu_reference(n_positions: int, threads: int):
     one(0)  # warm-up
     t0 = time.perf_counter()
     with ThreadPoolExecutor(threads) as ex:
-        list(ex.map(one, range(len(positions))))
+        vals = list(ex.map(one, range(len(positions))))
     dt = time.perf_counter() - t0
-    return len(positions) * len(p.thicknesses) / dt, dt, len(positions)
+    out = (len(positions) * len(p.thicknesses) / dt, dt, len(positions))
+    if want_values:
+        return out + ([np.array([v[d][0] for v in vals]) for d in range(len(dets))],)
+    return out
 
 
 def run_reference(args):
@@ -205,6 +218,7 @@ def main():
     ap.add_argument("--cpu-positions", type=int, default=32)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -332,13 +346,39 @@ def main():
         engine.apply(opts)
         engine.set_stream(stream.cuda_stream)
 
+    # every form on the same scan (one timed scan each after a warm-up), for the metric's form comparison
+    forms, form_values = {}, {}
+    if rank == 0 and world == 1 and not args.no_forms:
+        for f in ("plain", "fused", "bf16x3"):
+            engine.apply(sk.ExecutionOptions(form=f, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma))
+            engine.set_stream(stream.cuda_stream)
+            scan_once()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            scan_once()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fms = e0.elapsed_time(e1)
+            forms[f] = {"value": steps_per_scan / (fms / 1e3), "ms_per_scan": fms}
+            form_values[f] = [o.cpu().numpy().copy() for o in outs]
+        engine.apply(opts)
+        engine.set_stream(stream.cuda_stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = min(8, os.cpu_count() or 1)
-        v, dt, n = cpu_reference(args.cpu_positions, threads)
+        v, dt, n, ref_vals = cpu_reference(args.cpu_positions, threads, want_values=True)
         cpu = {"value": v, "unit": "probe.slice steps/s", "cores": threads, "kind": "port",
                "sample": f"{n} of 4096 positions x 20 slices ({dt:.1f} s), float64 NumPy restatement of STEM.cpuScan, "
                          f"{threads} threads over positions"}
+        idx = sample_indices(args.cpu_positions)
+        for f, vals in form_values.items():
+            errs = [float(np.linalg.norm(vals[d][idx] - ref_vals[d]) / np.linalg.norm(ref_vals[d]))
+                    for d in range(len(dets))]
+            forms[f]["rel_l2_vs_fp64"] = dict(zip([name for name, _, _ in DETECTORS], errs))
+        if forms:
+            forms["error_sample"] = f"detector values at the {n} CPU sample positions vs the float64 oracle"
 
     if rank == 0:
         line = {"metric": "probe.slice steps/s", "value": value, "unit": "probe.slice steps/s", "n_gpus": world,
@@ -350,7 +390,8 @@ def main():
                            "positions": n_pos, "slices": 20,
                            "grid": [NX, NY], "replicas": world, "l2": "inputs larger than L2 (batch of waves up to "
                                                                      "1 GiB per launch)"},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu, "forms": forms or None, "clocks": clocks.summary(),
+                "gpu_launches": launches,
                 "e2e": {"value": e2e_val, "unit": "probe.slice steps/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h}}
         print(json.dumps(line), flush=True)
