@@ -44,6 +44,7 @@ extern "C" {
 #define SIMK_OPT_TIMING 4       /* record CUDA events around every hot-path launch (default 0) */
 #define SIMK_OPT_COL_TILE 5     /* columns per CTA in the fused column pass, 0 = automatic (default 0) */
 #define SIMK_OPT_TMA 6          /* TMA-pipelined persistent column pass where the grid allows it (default 1) */
+#define SIMK_OPT_GRAPHS_CACHED 7 /* read-only: slice loops held as instantiated CUDA graphs */
 
 /* ---- Lobato pi choice (LobatoParameterization.PiConstant, LobatoParameterization.swift:15-24) ---- */
 #define SIMK_PI_EXACT 0

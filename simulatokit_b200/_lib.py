@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "libsimulato_cuda.so")
 SIMK_OK, SIMK_ERR_INVALID, SIMK_ERR_CUDA, SIMK_ERR_UNAVAILABLE, SIMK_ERR_MEMORY, SIMK_ERR_TIMEOUT = range(6)
 FORM_PLAIN, FORM_FUSED, FORM_BF16X3 = 0, 1, 2
 OPT_FORM, OPT_BATCH, OPT_BATCH_BYTES, OPT_GRAPHS, OPT_TIMING, OPT_COL_TILE, OPT_TMA = 0, 1, 2, 3, 4, 5, 6
+OPT_GRAPHS_CACHED = 7
 PI_EXACT, PI_ABTEM_FLOAT32 = 0, 1
 DET_ANNULAR, DET_PIXELATED, DET_COM, DET_SEGMENTED = 0, 1, 2, 3
 MAXANGLE_CUTOFF, MAXANGLE_VALID, MAXANGLE_FULL = 0, 1, 2

@@ -136,7 +136,10 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                 break;
             case SIMK_OPT_BATCH: SIMK_REQUIRE(value >= 0, "batch must be >= 0"); c.batch = value; break;
             case SIMK_OPT_BATCH_BYTES: c.batch_bytes = std::max<int64_t>(1, value); break;
-            case SIMK_OPT_GRAPHS: c.graphs = value ? 1 : 0; break;
+            case SIMK_OPT_GRAPHS:
+                c.graphs = value ? 1 : 0;
+                if (!c.graphs) c.drop_graphs();
+                break;
             case SIMK_OPT_TIMING:
                 c.timing = value ? 1 : 0;
                 if (c.timing) c.times.reserve(16384);
@@ -186,6 +189,7 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_TIMING: *value = c.timing; break;
             case SIMK_OPT_COL_TILE: *value = c.col_tile; break;
             case SIMK_OPT_TMA: *value = c.tma; break;
+            case SIMK_OPT_GRAPHS_CACHED: *value = (int64_t)c.slice_graphs.size(); break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });

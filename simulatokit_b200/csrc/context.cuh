@@ -1,6 +1,10 @@
 // context.cuh -- the library's context (stream, options, plan and table caches) and its potential handle.
 #pragma once
 
+#include <map>
+#include <set>
+#include <string>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -125,6 +129,21 @@ struct Context {
     // per-scan set-up kept across calls: detector maps by (grid, energy, detectors), spectra by (grid, probe)
     std::map<std::string, std::unique_ptr<DetectorPlan>> detector_plans;
     std::map<std::string, std::unique_ptr<DeviceBuffer>> spectra;
+    // The fused form's slice loop of a batch, captured as a CUDA graph on its second use (the first runs eagerly and
+    // creates what the launches need), keyed by every pointer and setting the recorded launches read.
+    struct SliceGraph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+    };
+    std::map<std::string, SliceGraph> slice_graphs;
+    std::set<std::string> slice_seen;
+    void drop_graphs() {
+        for (auto& kv : slice_graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        slice_graphs.clear();
+        slice_seen.clear();
+    }
+    ~Context() { drop_graphs(); }
 
     const LinePlan& plan(int n, int precision) {
         auto key = std::make_pair(n, precision);

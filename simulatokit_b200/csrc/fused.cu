@@ -950,8 +950,78 @@ bool fused_supported(Context& ctx, const GridGeom& g) {
     return choose(g.nx).E != 0 && choose(g.ny).E != 0;
 }
 
+namespace {
+void propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi,
+                           int count, bool probe_rows_pending, const std::function<void(int, bool)>& on_slice,
+                           bool kspace_last);
+
+template <typename T> void key_append(std::string& k, const T& v) {
+    k.append(reinterpret_cast<const char*>(&v), sizeof(T));
+}
+}  // namespace
+
+// The slice loop of one batch: 2 launches per slice. With SIMK_OPT_GRAPHS (and no per-kernel timing, no per-slice
+// callback) the loop is replayed from a CUDA graph: the first time a key is seen it runs eagerly (creating the
+// propagators, the error flag and the launch configurations), the second time it is captured and instantiated, and
+// from then on one graph launch replaces the 2 S kernel launches. The key holds every pointer and setting the
+// recorded launches read, so a replay never sees a freed or different buffer.
 void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
                      bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last) {
+    if (!ctx.graphs || ctx.timing || on_slice) {
+        propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, on_slice, kspace_last);
+        return;
+    }
+    std::string key;
+    key_append(key, psi);
+    key_append(key, count);
+    key_append(key, pot.t.ptr);
+    key_append(key, pot.g.nx);
+    key_append(key, pot.g.ny);
+    key_append(key, probe_rows_pending);
+    key_append(key, kspace_last);
+    key_append(key, ctx.form);
+    key_append(key, ctx.col_tile);
+    key_append(key, ctx.tma);
+    key_append(key, ctx.stream);
+    for (int j = 0; j < pot.n_slices(); ++j) key_append(key, ctx.propagator(pot.g, energy, pot.dz[j], tx, ty).p.ptr);
+    auto it = ctx.slice_graphs.find(key);
+    if (it != ctx.slice_graphs.end()) {
+        SIMK_CUDA(cudaGraphLaunch(it->second.exec, ctx.stream));
+        ctx.launches += it->second.launches;
+        return;
+    }
+    if (ctx.slice_seen.insert(key).second) {
+        propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, nullptr, kspace_last);
+        return;
+    }
+    if (ctx.slice_graphs.size() >= 64) ctx.drop_graphs();
+    const int64_t before = ctx.launches;
+    cudaGraph_t graph = nullptr;
+    SIMK_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, nullptr, kspace_last);
+    } catch (...) {
+        cudaStreamEndCapture(ctx.stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        ctx.launches = before;
+        throw;
+    }
+    SIMK_CUDA(cudaStreamEndCapture(ctx.stream, &graph));
+    const int64_t n = ctx.launches - before;
+    ctx.launches = before;
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    SIMK_CUDA(e);
+    ctx.slice_graphs[key] = Context::SliceGraph{exec, n};
+    SIMK_CUDA(cudaGraphLaunch(exec, ctx.stream));
+    ctx.launches += n;
+}
+
+namespace {
+void propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi,
+                           int count, bool probe_rows_pending, const std::function<void(int, bool)>& on_slice,
+                           bool kspace_last) {
     const GridGeom& g = pot.g;
     const long long N = g.count();
     const RegPlan prow = reg_plan(ctx, g.ny);
@@ -981,6 +1051,8 @@ void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx,
         if (on_slice) on_slice(j, last && kspace_last);
     }
 }
+
+}  // namespace
 
 // The waves after slice j are in "row spectrum" form (columns inverse-transformed, rows not): the row IFFT that
 // completes them, in place.

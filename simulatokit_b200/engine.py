@@ -87,6 +87,12 @@ class Engine:
         L.check(self.lib.simk_context_launch_count(self.handle, C.byref(v), 1 if reset else 0))
         return int(v.value)
 
+    def graphs_cached(self) -> int:
+        """Slice loops the context holds as instantiated CUDA graphs."""
+        v = C.c_int64(0)
+        L.check(self.lib.simk_context_get_option(self.handle, L.OPT_GRAPHS_CACHED, C.byref(v)))
+        return int(v.value)
+
     def set_timing(self, on: bool):
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TIMING, 1 if on else 0))
 
