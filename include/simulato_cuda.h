@@ -55,6 +55,12 @@ extern "C" {
 #define SIMK_DET_PIXELATED 1
 #define SIMK_DET_COM 2
 #define SIMK_DET_SEGMENTED 3
+/* No reference counterpart (its PixelatedDetector offers cutoff / valid / full only, Detectors.swift:140-168): the
+ * pattern on a uniform nr x nphi grid of angles over [-outer, outer) mrad in x and y (bin 0 at -outer). Each k-space
+ * pixel is a square of one angular sample centred on its angle; its intensity goes to the bins it overlaps in
+ * proportion to the overlap area, so the total inside the window is conserved. outer must not exceed the largest
+ * simulated angle along either axis. */
+#define SIMK_DET_BINNED 4
 #define SIMK_MAXANGLE_CUTOFF 0   /* PixelatedDetector.MaxAngle */
 #define SIMK_MAXANGLE_VALID 1
 #define SIMK_MAXANGLE_FULL 2
@@ -89,7 +95,8 @@ typedef struct {
 } simk_probe;
 
 /* One detector (Detectors.swift:91-263). annular: inner, outer (has_outer = 0: the default outer angle);
- * pixelated: max_angle; com: max_angle, units; segmented: nr, nphi, inner, outer, rotation [rad]. */
+ * pixelated: max_angle; com: max_angle, units; segmented: nr, nphi, inner, outer, rotation [rad]; binned: nr x nphi
+ * bins (x, y), outer = the window's half-width [mrad]. */
 typedef struct {
     int32_t kind;
     int32_t max_angle;

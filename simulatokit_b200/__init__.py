@@ -7,8 +7,8 @@ every compute call raises CudaUnavailable."""
 
 from ._lib import CudaFailure, CudaUnavailable, InvalidArgument, SimulatoError  # noqa: F401
 from .core import Antialias, AtomicStructure, ElectronBeam, Grid, Waves  # noqa: F401
-from .detector import (STEM, AnnularDetector, CenterOfMassDetector, PixelatedDetector, ScanMeasurement,  # noqa: F401
-                       SegmentedDetector, detector_shape)
+from .detector import (STEM, AnnularDetector, BinnedPixelatedDetector, CenterOfMassDetector,  # noqa: F401
+                       PixelatedDetector, ScanMeasurement, SegmentedDetector, detector_shape)
 from .engine import Engine, ExecutionOptions  # noqa: F401
 from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, LobatoParameterization,  # noqa: F401
                          Multislice, Potential, ProjectedPotential, Slicing, Surrogate, finite_profile)

@@ -34,6 +34,12 @@ struct DetectorPlan {
     long long total_entries = 0;
     long long total_crop = 0;
     std::vector<int> host_chan_ptr;
+    // binned detectors: per axis, each bin's (pixel, overlap weight) list in CSR form
+    struct Binned {
+        int det = 0, nbx = 0, nby = 0;
+        DeviceBuffer xp, xi, xw, yp, yi, yw;  // int32 ptr [nb + 1], int32 pixel, float64 weight
+    };
+    std::vector<std::unique_ptr<Binned>> binned;
 };
 
 struct Propagator {

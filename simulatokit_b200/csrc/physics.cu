@@ -535,6 +535,7 @@ void detector_shape(const GridGeom& g, double energy, const simk_detector& d, in
         }
         case SIMK_DET_COM: *ndim = 1; shape[0] = 2; break;
         case SIMK_DET_SEGMENTED: *ndim = 2; shape[0] = d.nr; shape[1] = d.nphi; break;
+        case SIMK_DET_BINNED: *ndim = 2; shape[0] = d.nr; shape[1] = d.nphi; break;
         default: throw Error(SIMK_ERR_INVALID, "unknown detector kind");
     }
 }
@@ -626,6 +627,47 @@ std::unique_ptr<DetectorPlan> build_detector_plan(Context& ctx, const GridGeom& 
             plan->det_first_channel.push_back((int)channels.size());
             plan->det_pixelated_offset.push_back(-1);
             for (auto& b : bins) channels.push_back(std::move(b));
+        } else if (d.kind == SIMK_DET_BINNED) {
+            SIMK_REQUIRE(d.nr >= 1 && d.nphi >= 1 && d.nr <= 4096 && d.nphi <= 4096, "bins must be in 1..4096");
+            const double wmax = std::min((g.nx / 2) * a.ax, (g.ny / 2) * a.ay);
+            SIMK_REQUIRE(std::isfinite(d.outer) && d.outer > 0 && d.outer <= wmax,
+                         "the binned window must lie within the largest simulated angle (" + std::to_string(wmax) +
+                             " mrad)");
+            auto b = std::make_unique<DetectorPlan::Binned>();
+            b->det = di;
+            b->nbx = d.nr;
+            b->nby = d.nphi;
+            // per axis: bin k covers [-outer + k w, -outer + (k + 1) w), pixel i covers [alpha_i - s/2, alpha_i + s/2)
+            auto axis = [&](int n, double samp, int nb, DeviceBuffer& P, DeviceBuffer& I, DeviceBuffer& W) {
+                const std::vector<double> al = angles_of(n, samp);
+                const double bw = 2.0 * d.outer / nb;
+                std::vector<int> ptr(1, 0), idx;
+                std::vector<double> wt;
+                for (int k = 0; k < nb; ++k) {
+                    const double lo = -d.outer + k * bw, hi = lo + bw;
+                    for (int i = 0; i < n; ++i) {
+                        const double ov = std::min(hi, al[i] + 0.5 * samp) - std::max(lo, al[i] - 0.5 * samp);
+                        if (ov > 0) {
+                            idx.push_back(i);
+                            wt.push_back(ov / samp);
+                        }
+                    }
+                    ptr.push_back((int)idx.size());
+                }
+                P.alloc(ptr.size() * sizeof(int));
+                SIMK_CUDA(cudaMemcpy(P.ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+                I.alloc(std::max<size_t>(1, idx.size()) * sizeof(int));
+                W.alloc(std::max<size_t>(1, wt.size()) * sizeof(double));
+                if (!idx.empty()) {
+                    SIMK_CUDA(cudaMemcpy(I.ptr, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice));
+                    SIMK_CUDA(cudaMemcpy(W.ptr, wt.data(), wt.size() * sizeof(double), cudaMemcpyHostToDevice));
+                }
+            };
+            axis(g.nx, a.ax, d.nr, b->xp, b->xi, b->xw);
+            axis(g.ny, a.ay, d.nphi, b->yp, b->yi, b->yw);
+            plan->det_first_channel.push_back(-1);
+            plan->det_pixelated_offset.push_back(-1);
+            plan->binned.push_back(std::move(b));
         } else {
             throw Error(SIMK_ERR_INVALID, "unknown detector kind");
         }
@@ -706,6 +748,33 @@ __global__ void k_detect_pixelated(const float2* __restrict__ phi, long long N, 
     }
 }
 
+// Binned detector: one thread per (position, bin), the separable overlap weights over the bin's pixels summed in
+// float64 in a fixed order.
+__global__ void k_detect_binned(const float2* __restrict__ phi, long long N, int ny, const int* __restrict__ xp,
+                                const int* __restrict__ xi, const double* __restrict__ xw, const int* __restrict__ yp,
+                                const int* __restrict__ yi, const double* __restrict__ yw, int nbx, int nby,
+                                double* out, long long first_position, int count, double weight, float iscale) {
+    const long long m = (long long)nbx * nby;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m * count;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(i / m);
+        const long long o = i - (long long)b * m;
+        const int bx = (int)(o / nby), by = (int)(o - (long long)bx * nby);
+        const float2* w = phi + (long long)b * N;
+        double s = 0.0;
+        for (int p = xp[bx]; p < xp[bx + 1]; ++p) {
+            const long long row = (long long)xi[p] * ny;
+            double sy = 0.0;
+            for (int q = yp[by]; q < yp[by + 1]; ++q) {
+                const float2 v = w[row + yi[q]];
+                sy += yw[q] * (double)((v.x * v.x + v.y * v.y) * iscale);
+            }
+            s += xw[p] * sy;
+        }
+        out[(first_position + b) * m + o] += weight * s;
+    }
+}
+
 void launch_detect(Context& ctx, const DetectorPlan& plan, const GridGeom& g, const float2* phi, int count,
                    long long first_position, double* const* outputs_dev, double weight, float intensity_scale) {
     const long long N = g.count();
@@ -731,6 +800,13 @@ void launch_detect(Context& ctx, const DetectorPlan& plan, const GridGeom& g, co
         k_detect_pixelated<<<blocks_for((long long)m * count), 256, 0, ctx.stream>>>(
             phi, N, plan.crop_src.as<int>() + plan.det_pixelated_offset[d], m, outputs_dev[d], first_position, count,
             weight, intensity_scale);
+        ++ctx.launches;
+    }
+    for (const auto& b : plan.binned) {
+        const long long m = (long long)b->nbx * b->nby;
+        k_detect_binned<<<blocks_for(m * count), 256, 0, ctx.stream>>>(
+            phi, N, g.ny, b->xp.as<int>(), b->xi.as<int>(), b->xw.as<double>(), b->yp.as<int>(), b->yi.as<int>(),
+            b->yw.as<double>(), b->nbx, b->nby, outputs_dev[b->det], first_position, count, weight, intensity_scale);
         ++ctx.launches;
     }
     SIMK_CUDA(cudaGetLastError());

@@ -76,6 +76,23 @@ class SegmentedDetector:
                             float(self.rotation))
 
 
+class BinnedPixelatedDetector:
+    """The pattern on a uniform gpts[0] x gpts[1] grid of angles over [-max_angle, max_angle) mrad per axis, bin 0 at
+    -max_angle: each k-space pixel's intensity goes to the bins its square overlaps, in proportion to the overlap area.
+    The reference's PixelatedDetector has no numeric-angle mode (Detectors.swift:140-168; only cutoff / valid / full),
+    so this rule is this library's own: 4D-STEM patterns "cropped to 128 x 128 up to 60 mrad"."""
+
+    def __init__(self, max_angle: float, gpts=(128, 128)):
+        if not (math.isfinite(max_angle) and max_angle > 0):
+            _refuse("the maximum angle must be finite and positive")
+        if len(gpts) != 2 or min(gpts) < 1 or max(gpts) > 4096:
+            _refuse("bins must be in 1..4096 per axis")
+        self.max_angle, self.gpts = float(max_angle), (int(gpts[0]), int(gpts[1]))
+
+    def c(self):
+        return L.Detector_t(L.DET_BINNED, 0, 0, 1, self.gpts[0], self.gpts[1], 0.0, self.max_angle, 0.0)
+
+
 def detector_shape(detector, grid: Grid, energy: float):
     g = grid.c()
     d = detector.c()
