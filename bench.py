@@ -56,6 +56,64 @@ def srtio3(nx, ny, nz):
     return (nx * A0, ny * A0, nz * A0), np.tile(nums, len(shifts)), pos
 
 
+def silicon(nx, ny, nz, a0=5.431):
+    """Diamond-cubic Si: the 8 atoms of the conventional cell, x outermost (AtomicStructure.repeated's order)."""
+    frac = np.array([(0, 0, 0), (0, 0.5, 0.5), (0.5, 0, 0.5), (0.5, 0.5, 0), (0.25, 0.25, 0.25), (0.25, 0.75, 0.75),
+                     (0.75, 0.25, 0.75), (0.75, 0.75, 0.25)], dtype=np.float64)
+    shifts = np.array([(i, j, k) for i in range(nx) for j in range(ny) for k in range(nz)], dtype=np.float64)
+    pos = ((shifts[:, None, :] + frac[None, :, :]) * a0).reshape(-1, 3)
+    return (nx * a0, ny * a0, nz * a0), np.full(len(pos), 14), pos
+
+
+def amorphous(box, n_atoms, dmin, species, seed):
+    """Random positions in `box` with a minimum separation `dmin` (periodic in x and y), by sequential addition on a
+    cell grid of side >= dmin; Z drawn from `species` {Z: probability}. Deterministic for a seed."""
+    rng = np.random.default_rng(seed)
+    box = np.asarray(box, dtype=np.float64)
+    nc = np.maximum(1, np.floor(box / dmin).astype(int))
+    side = box / nc
+    cells = -np.ones(tuple(nc) + (8,), dtype=np.int64)
+    fill = np.zeros(tuple(nc), dtype=np.int64)
+    pos = np.empty((n_atoms, 3))
+    n = 0
+    d2 = dmin * dmin
+    while n < n_atoms:
+        cand = rng.uniform(0, 1, (4096, 3)) * box
+        for p in cand:
+            c = np.minimum((p / side).astype(int), nc - 1)
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        cz = c[2] + dz
+                        if cz < 0 or cz >= nc[2]:
+                            continue
+                        cx, cy = (c[0] + dx) % nc[0], (c[1] + dy) % nc[1]
+                        for k in range(fill[cx, cy, cz]):
+                            q = pos[cells[cx, cy, cz, k]]
+                            d = p - q
+                            d[:2] -= np.round(d[:2] / box[:2]) * box[:2]
+                            if d @ d < d2:
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok and fill[c[0], c[1], c[2]] < 8:
+                pos[n] = p
+                cells[c[0], c[1], c[2], fill[c[0], c[1], c[2]]] = n
+                fill[c[0], c[1], c[2]] += 1
+                n += 1
+                if n == n_atoms:
+                    break
+    zs = np.array(sorted(species))
+    nums = rng.choice(zs, n_atoms, p=[species[z] for z in zs])
+    return tuple(box), nums, pos
+
+
 def scan_positions():
     xs = np.arange(SCAN_N) * (A0 / SCAN_N) + 4 * A0
     return np.stack(np.meshgrid(xs, xs, indexing="ij"), axis=-1).reshape(-1, 2)
@@ -202,6 +260,199 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------------------------------------------------
+# Further workloads (--workload 4dstem | surrogate): the same measurement on the other scan configurations
+# ---------------------------------------------------------------------------------------------------------------------
+
+def _device_scan(sk, L, engine, probe, pots, positions, dets, torch):
+    """A callable running simk_scan_device over `positions` (device-resident) for `pots`, and its output buffers."""
+    import ctypes as C
+    handles = [p.handle(engine) for p in pots]
+    n_pos = len(positions)
+    pos_dev = torch.tensor(positions, dtype=torch.float64, device="cuda")
+    counts = [int(np.prod(sk.detector_shape(d, probe.grid, probe.beam.energy) or [1])) for d in dets]
+    outs = [torch.zeros(n_pos * c, dtype=torch.float64, device="cuda") for c in counts]
+    harr = (C.c_void_p * len(handles))(*[h.handle for h in handles])
+    darr = (L.Detector_t * len(dets))(*[d.c() for d in dets])
+    oarr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+    pc = probe.c()
+
+    def run():
+        L.check(engine.lib.simk_scan_device(engine.handle, C.byref(pc), len(handles), harr, n_pos,
+                                            C.c_void_p(pos_dev.data_ptr()), len(dets), darr, oarr))
+    return run, outs
+
+
+def _time_scans(engine, run, steps, warmup, stream, torch, local):
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    engine.launch_count(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = engine.launch_count()
+    # per-kernel durations from a second, event-instrumented pass
+    engine.set_timing(True)
+    engine.kernel_time("fused_cols", reset=True)
+    run()
+    torch.cuda.synchronize()
+    names = ["fused_rows", "fused_cols", "line_fft", "pointwise", "detect"]
+    kt = {n: engine.kernel_time(n) for n in names}
+    engine.set_timing(False)
+    return ms, launches, clocks.summary(), kt
+
+
+def _roofline(kt, n):
+    dom = max(kt, key=lambda k: kt[k][0])
+    dms, dn, dbytes = kt[dom]
+    peak, kind = measured_peaks()
+    achieved = (dbytes / dn) / (dms / dn / 1e3) / 1e9 if dn else None
+    total = sum(v[0] for v in kt.values())
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "fallback 6.65 TB/s",
+            "traffic": None, "algorithmic_bytes_per_launch": dbytes / dn if dn else None,
+            "avg_launch_ms": dms / dn if dn else None,
+            "kernel_share": {k: round(v[0] / total, 4) for k, v in kt.items() if v[1]},
+            "step_bytes_rule": f"32*N bytes per probe.slice step, N = {n}x{n}"}
+
+
+def run_4dstem(args, sk, L, engine, stream, torch, local):
+    """4D-STEM with frozen phonons: Si 6x6x20, 768^2, 80 slices, 16 configurations, 48x48 scan, binned 128x128 up to
+    60 mrad + COM (mrad)."""
+    a = 5.431
+    box, nums, pos = silicon(6, 6, 20)
+    st = sk.AtomicStructure(box, nums, pos)
+    fp = sk.FrozenPhonons(st, sigmas={14: 0.075}, configurations=16, seed=1)
+    pots = [sk.Potential(fp.configuration(c), 768, 768, slice_thickness=1.35775) for c in range(fp.count)]
+    assert pots[0].slice_count == 80
+    probe = sk.Probe(sk.ElectronBeam(300e3), pots[0].grid, sk.Aperture(25.0), sk.Aberrations(C10=-50.0))
+    scan = sk.GridScan((3 * a, 3 * a), (4 * a, 4 * a), 48, 48)
+    dets = [sk.BinnedPixelatedDetector(60.0, (128, 128)), sk.CenterOfMassDetector("valid", "mrad")]
+    positions = np.asarray(scan.positions)
+    run, outs = _device_scan(sk, L, engine, probe, pots, positions, dets, torch)
+    ms, launches, clocks, kt = _time_scans(engine, run, args.steps, args.warmup, stream, torch, local)
+    steps = len(positions) * 80 * len(pots)
+    value = steps * args.steps / (ms / 1e3)
+    cpu, errs = None, None
+    if not args.no_cpu:
+        # the oracle on config 0 at 2 positions (bounded sample), and the device's single-configuration values there
+        from oracle import simk_oracle as O
+        idx = [0, len(positions) // 2 + 24]
+        x = fp.configuration(0)
+        op = O.Potential.from_structure(O.Structure(x.box, x.numbers, x.positions), 768, 768, slice_thickness=1.35775)
+        t0 = time.perf_counter()
+        ref = O.stem_scan(O.ProbeSpec(300e3, 25.0, {"C10": -50.0}), [(op.grid, op.build(), op.thicknesses)],
+                          positions[idx], [O.DetectorSpec("binned", {"nbx": 128, "nby": 128, "outer": 60.0}),
+                                           O.DetectorSpec("com", {"mode": "valid", "units": "mrad"})])
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(idx) * 80 / dt, "unit": "probe.slice steps/s", "cores": 1, "kind": "port",
+               "sample": f"{len(idx)} positions x 80 slices of configuration 0 ({dt:.1f} s incl. its potential), "
+                         "float64 NumPy restatement"}
+        one, o1 = _device_scan(sk, L, engine, probe, pots[:1], positions[idx], dets, torch)
+        one()
+        torch.cuda.synchronize()
+        errs = {"binned": float(np.linalg.norm(o1[0].cpu().numpy() - ref[0].ravel()) / np.linalg.norm(ref[0])),
+                "com": float(np.linalg.norm(o1[1].cpu().numpy() - ref[1].ravel()) / np.linalg.norm(ref[1]))}
+    return {"metric": "probe.slice steps/s", "value": value, "ms_per_step": ms / args.steps,
+            "config": {"workload": "4D-STEM with frozen phonons, Si 6x6x20 (5760 atoms, 108.6 A), 768x768, 80 slices "
+                                   "of 1.35775 A, 16 configurations (sigma 0.075 A, seed 1), 300 keV, 25 mrad, "
+                                   "C10 = -50 A, 48x48 scan over one unit cell, binned 128x128 up to 60 mrad + COM",
+                       "form": args.form, "steps_per_scan": steps},
+            "roofline": _roofline(kt, 768), "cpu_baseline": cpu, "rel_l2_vs_fp64": errs, "clocks": clocks,
+            "gpu_launches": launches}
+
+
+def run_surrogate(args, sk, L, engine, stream, torch, local):
+    """The learned potential surrogate feeding a HAADF scan: amorphous 50x50x100 A (25,000 atoms, min separation
+    1.4 A, Z from {6: 0.7, 8: 0.2, 14: 0.08, 79: 0.02}), finite projection on 1024^2 with 100 slices of 1 A, built by
+    the quadrature and by the surrogate (trained on the device on quadrature-labelled samples); then a 32x32 HAADF
+    scan (200 keV, 20 mrad, 50-200 mrad) through the surrogate's potential."""
+    box, nums, pos = amorphous((50.0, 50.0, 100.0), 25000, 1.4, {6: 0.7, 8: 0.2, 14: 0.08, 79: 0.02}, seed=1)
+    st = sk.AtomicStructure(box, nums, pos)
+
+    def build(**kw):
+        p = sk.Potential(st, 1024, 1024, slice_thickness=1.0, projection="finite", **kw)
+        torch.cuda.synchronize()
+        engine.set_timing(True)
+        engine.kernel_time("finite_quadrature", reset=True)
+        t0 = time.perf_counter()
+        p.handle(engine)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        kq, ks = engine.kernel_time("finite_quadrature"), engine.kernel_time("surrogate_infer")
+        engine.set_timing(False)
+        return p, wall, kq[0], ks[0]
+
+    pq, wall_q, tq, _ = build()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sur = sk.Surrogate([6, 8, 14, 79], n_samples=args.sg_samples, steps=args.sg_steps, batch=4096, seed=1,
+                       engine=engine)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    ps, wall_s, tq_s, ts = build(surrogate=sur, error_bound=0.05)
+    vq = pq.build(engine).values
+    vs = ps.build(engine).values
+    pot_err = {"max_abs_over_max": float(np.max(np.abs(vs - vq)) / np.max(np.abs(vq))),
+               "rel_l2": float(np.linalg.norm(vs - vq) / np.linalg.norm(vq))}
+    del vq, vs
+    probe = sk.Probe(sk.ElectronBeam(200e3), pq.grid, sk.Aperture(20.0))
+    scan = sk.GridScan((20.0, 20.0), (30.0, 30.0), 32, 32)
+    positions = np.asarray(scan.positions)
+    dets = [sk.AnnularDetector(50.0, 200.0)]
+    run_s, out_s = _device_scan(sk, L, engine, probe, [ps], positions, dets, torch)
+    ms, launches, clocks, kt = _time_scans(engine, run_s, args.steps, args.warmup, stream, torch, local)
+    run_q, out_q = _device_scan(sk, L, engine, probe, [pq], positions, dets, torch)
+    run_q()
+    torch.cuda.synchronize()
+    haadf_err = float(torch.linalg.norm(out_s[0] - out_q[0]) / torch.linalg.norm(out_q[0]))
+    steps = len(positions) * 100
+    value = steps * args.steps / (ms / 1e3)
+    info = sur.info
+    return {"metric": "probe.slice steps/s", "value": value, "ms_per_step": ms / args.steps,
+            "config": {"workload": "amorphous 50x50x100 A (25,000 atoms, min separation 1.4 A, C/O/Si/Au "
+                                   "70/20/8/2 %), finite projection 1024x1024, 100 slices of 1 A, learned surrogate, "
+                                   "32x32 HAADF scan (50-200 mrad) at 200 keV, 20 mrad", "form": args.form,
+                       "steps_per_scan": steps},
+            "surrogate": {"train_s": train_s, "samples": args.sg_samples, "steps": args.sg_steps,
+                          "val_rms_dF": info.get("val_rms_rel"), "val_max_dF": info.get("val_max_rel"),
+                          "used": ps.used_surrogate, "judged_max_dP_over_Pinf": ps.judged_max_rel,
+                          "profile_tables_ms": {"quadrature": tq, "surrogate": ts},
+                          "potential_build_wall_s": {"quadrature": wall_q, "surrogate": wall_s},
+                          "potential_error_vs_quadrature": pot_err,
+                          "haadf_rel_l2_vs_quadrature_potential": haadf_err},
+            "roofline": _roofline(kt, 1024), "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches}
+
+
+def run_extra(args):
+    import torch
+    import simulatokit_b200 as sk
+    from simulatokit_b200 import _lib as L
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return  # one GPU: these workloads have no replica mode
+    torch.cuda.set_device(local)
+    engine = sk.Engine.require(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    engine.set_stream(stream.cuda_stream)
+    engine.apply(sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma))
+    fn = run_4dstem if args.workload == "4dstem" else run_surrogate
+    line = fn(args, sk, L, engine, stream, torch, local)
+    line.update({"unit": "probe.slice steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                 "data": "synthetic", "e2e": None})
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------------------------------------------------
 
@@ -219,9 +470,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
+    ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate"],
+                    help="stem: the headline STEM HAADF+BF scan; 4dstem and surrogate: the other scan configurations")
+    ap.add_argument("--sg-samples", type=int, default=10_000_000, help="surrogate workload: quadrature samples")
+    ap.add_argument("--sg-steps", type=int, default=20000, help="surrogate workload: training steps")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "stem":
+        run_extra(args)
         return
 
     import torch

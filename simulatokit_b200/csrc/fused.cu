@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "engine.cuh"
+#include "ccfft.cuh"
 #include "tcfft.cuh"
 #include "tma.cuh"
 
@@ -372,6 +373,23 @@ __device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool n
 // columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each.
 // ENG 0: register-resident float32 Cooley-Tukey passes; ENG 1: the tile is transformed in place in shared memory with
 // radix-16 tensor-core stages (tcfft.cuh, the bf16x3 form).
+// Height of the column pass's TMA boxes: the largest divisor of N that is at most 256 (the box limit).
+constexpr int tma_box_rows(int n) {
+    for (int h = 256; h > 1; --h)
+        if (n % h == 0) return h;
+    return 1;
+}
+// Rows per tile of the row pass: the largest power of two with RB N / 8 <= 256 threads.
+constexpr int rows_per_tile(int n) {
+    int r = 1;
+    while (2 * r * (n / 8) <= 256) r *= 2;
+    return r;
+}
+
+// State an engine keeps per thread: register twiddles (0), the DFT-16 fragments (1), nothing (2).
+template <int N, int ENG>
+using EngineState = std::conditional_t<ENG == 0, TwRegs<N>, std::conditional_t<ENG == 1, Dft16Frags, int>>;
+
 // Blocks per SM the tensor-core engine asks the compiler for: two when a block has at most 256 threads (at most 128
 // registers a thread), else one.
 constexpr int tc_min_blocks(int threads, int eng) { return (eng == 1 && threads <= 256) ? 2 : 1; }
@@ -384,7 +402,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
                                                                int count, const float2* __restrict__ tw, int* err) {
     extern __shared__ __align__(128) unsigned char smem_tma[];
     constexpr int T = N / 8;
-    constexpr int BOXH = N <= 256 ? N : 256;
+    constexpr int BOXH = tma_box_rows(N);
     constexpr int NBOX = N / BOXH;
     constexpr int TILE = N * TC;  // float2 per tile
     constexpr uint32_t STAGE_BYTES = 2u * TILE * sizeof(float2);
@@ -403,9 +421,9 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         abort_flag = 0;
     }
     __syncthreads();
-    [[maybe_unused]] std::conditional_t<ENG == 0, TwRegs<N>, Dft16Frags> eng;
+    [[maybe_unused]] EngineState<N, ENG> eng;
     if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
-    else eng = dft16_frags(tid & 31);
+    else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     auto issue = [&](unsigned tile, int s) {
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
@@ -445,6 +463,20 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, eng, sm);
 #pragma unroll
             for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
+        } else if constexpr (ENG == 2) {
+            using L = CcLayout<N, TC, true>;
+            float2* scratch = stages + 4 * TILE;
+            float2* out = cc_fft<N, TC, true, -1, PRE_NONE, true>(buf, scratch, nullptr, 1.0f, tw, tid);
+            if constexpr (MODE == 0) {
+                float2* other = (out == buf) ? scratch : buf;
+                out = cc_fft<N, TC, true, +1, PRE_MUL, false>(out, other, pbuf, pscale, tw, tid);
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                float2 v = out[L::at(c, (int)t + T * i)];
+                if constexpr (MODE == 1) v = cmul(v, pbuf[L::nat(c, (int)t + T * i)]) * pscale;
+                col[(size_t)(t + T * i) * ny] = v;
+            }
         } else {
             using L = TileLayout<N, TC, true>;
             float2* scratch = stages + 4 * TILE;
@@ -490,9 +522,9 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
         abort_flag = 0;
     }
     __syncthreads();
-    [[maybe_unused]] std::conditional_t<ENG == 0, TwRegs<N>, Dft16Frags> eng;
+    [[maybe_unused]] EngineState<N, ENG> eng;
     if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
-    else eng = dft16_frags(tid & 31);
+    else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     auto issue = [&](int tile, int s) {
         float2* dst = stages + s * 2 * TILE;
         const int row0 = tile * RB;
@@ -531,6 +563,29 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
             if (fwd) ct_fft_from<N, 0, -1>(v, t, eng, sm);
 #pragma unroll
             for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
+        } else if constexpr (ENG == 2) {
+            using L = CcLayout<N, RB, false>;
+            float2* scratch = stages + 4 * TILE;
+            float2* out = buf;
+            if (inv) out = cc_fft<N, RB, false, +1, PRE_NONE, true>(buf, scratch, nullptr, 1.0f, tw, tid);
+            if (fwd) {
+                float2* other = (out == buf) ? scratch : buf;
+                if (inv) {
+                    if (with_t) out = cc_fft<N, RB, false, -1, PRE_MUL, false>(out, other, tbuf, scale, tw, tid);
+                    else out = cc_fft<N, RB, false, -1, PRE_SCALE, false>(out, other, nullptr, scale, tw, tid);
+                } else {
+                    if (with_t) out = cc_fft<N, RB, false, -1, PRE_MUL, true>(out, other, tbuf, scale, tw, tid);
+                    else out = cc_fft<N, RB, false, -1, PRE_SCALE, true>(out, other, nullptr, scale, tw, tid);
+                }
+            }
+            const bool moved = inv || fwd;  // a transform ran: the tile is in the working layout
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int idx = (int)t + T * i;
+                float2 v = out[moved ? L::at(rr, idx) : L::nat(rr, idx)];
+                if (!fwd) v = with_t ? cmul(v, tbuf[L::nat(rr, idx)]) * scale : v * scale;
+                row[idx] = v;
+            }
         } else {
             using L = TileLayout<N, RB, false>;
             float2* scratch = stages + 4 * TILE;
@@ -700,10 +755,10 @@ template <int N, int ENG>
 bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
                      int fwd, float scale) {
     constexpr int T = N / 8;
-    constexpr int RB = (256 / T) > 0 ? (256 / T) : 1;
+    constexpr int RB = rows_per_tile(N);
     if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
-    // two stages of (rows, t rows), plus the tensor-core engine's scratch tile
-    const size_t smem = (ENG == 1 ? 5 : 4) * (size_t)N * RB * sizeof(float2);
+    // two stages of (rows, t rows), plus the shared-memory engines' scratch tile
+    const size_t smem = (ENG != 0 ? 5 : 4) * (size_t)N * RB * sizeof(float2);
     auto kern = fused_rows_tma<N, RB, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
@@ -724,9 +779,9 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
 template <int N, int TC, int MODE, int ENG>
 bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     constexpr int T = N / 8;
-    constexpr int BOXH = N <= 256 ? N : 256;
-    // two stages of (wave tile, P tile), plus the tensor-core engine's scratch tile
-    const size_t smem = (ENG == 1 ? 5 : 4) * (size_t)N * TC * sizeof(float2);
+    constexpr int BOXH = tma_box_rows(N);
+    // two stages of (wave tile, P tile), plus the shared-memory engines' scratch tile
+    const size_t smem = (ENG != 0 ? 5 : 4) * (size_t)N * TC * sizeof(float2);
     auto kern = fused_cols_tma<N, TC, MODE, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
@@ -872,6 +927,52 @@ bool cols_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     }
 }
 
+// ---- the float32 fused form at lengths that are not powers of two: the TMA passes with the shared-memory engine -----
+bool rows_cc(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv, int fwd,
+             float scale) {
+    switch (p.n) {
+        case 384: return launch_rows_tma<384, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 640: return launch_rows_tma<640, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 768: return launch_rows_tma<768, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 1536: return launch_rows_tma<1536, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        default: return false;
+    }
+}
+
+template <int N>
+bool cols_cc_n(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
+    for (; tc >= 2; tc /= 2) {
+        switch (tc) {
+            case 8:
+                if constexpr (8 * (N / 8) <= 1024) {
+                    if (launch_cols_tma<N, 8, 2>(ctx, p, a, count)) return true;
+                }
+                break;
+            case 4:
+                if constexpr (4 * (N / 8) <= 1024) {
+                    if (launch_cols_tma<N, 4, 2>(ctx, p, a, count)) return true;
+                }
+                break;
+            case 2:
+                if (launch_cols_tma<N, 2, 2>(ctx, p, a, count)) return true;
+                break;
+            default: break;
+        }
+    }
+    return false;
+}
+
+bool cols_cc(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    const int tc = ctx.col_tile > 0 ? ctx.col_tile : 4;
+    switch (p.n) {
+        case 384: return cols_cc_n<384>(ctx, p, a, count, tc);
+        case 640: return cols_cc_n<640>(ctx, p, a, count, tc);
+        case 768: return cols_cc_n<768>(ctx, p, a, count, tc);
+        case 1536: return cols_cc_n<1536>(ctx, p, a, count, tc);
+        default: return false;
+    }
+}
+
 bool tc_length(int n) { return n == 256 || n == 512 || n == 768 || n == 1024 || n == 2048; }
 
 void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
@@ -883,6 +984,7 @@ void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul
         return;
     }
     if (rows_ct(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return;
+    if (ctx.tma && rows_cc(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return;
     switch (p.E) {
         case 8: launch_rows_e<8>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
         case 12: launch_rows_e<12>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale); break;
@@ -902,6 +1004,7 @@ void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
         return;
     }
     if (cols_ct(ctx, p, a, count)) return;
+    if (ctx.tma && a.mode != 2 && cols_cc(ctx, p, a, count)) return;
     switch (p.E) {
         case 8: launch_cols_e<8>(ctx, p, a, count); break;
         case 12: launch_cols_e<12>(ctx, p, a, count); break;

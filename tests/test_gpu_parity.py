@@ -259,3 +259,18 @@ def test_refusals(engine):
     other = sk.Grid(64, 64, 10.0, 10.0)
     with pytest.raises(sk.InvalidArgument):
         sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), other), pot, engine=engine)
+
+
+@pytest.mark.parametrize("nx,ny", [(384, 384), (640, 384), (768, 768), (1536, 1536)])
+def test_fused_mixed_radix_lengths(engine, nx, ny):
+    """The fused form's TMA passes with the float32 shared-memory engine (radix 8/4/2 then 3 or 5) at grid sides that
+    are not powers of two: exit wave of a plane wave through SrTiO3 2x2x2 (4 slices) <= 1e-5 relative L2."""
+    s = O.srtio3_cell().repeated(2, 2, 2)
+    op = O.Potential.from_structure(s, nx, ny, slice_thickness=1.9525)
+    og = op.grid
+    ts = [O.transmission(v, 200e3, og) for v in op.build()]
+    ref = O.multislice(O.plane_wave(og), ts, op.thicknesses, 200e3, og)[-1]
+    pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), nx, ny, slice_thickness=1.9525)
+    ex = sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), pot.grid), pot,
+                           options=sk.ExecutionOptions(form="fused"), engine=engine)[-1]
+    assert O.rel_l2(ex.field, ref) <= 1e-5
