@@ -216,6 +216,28 @@ int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_poten
                      simk_potential* const* potentials, int32_t n_positions, const double* positions_xy_device,
                      int32_t n_detectors, const simk_detector* detectors, double* const* outputs_device);
 
+/* ---- job tables ----------------------------------------------------------------------------------------------------
+ * No reference counterpart as one call (the reference runs such jobs one Multislice.run at a time, Multislice.swift:52-80
+ * -> MetalEngine.swift:458-474); proposed as simk_job_table_run for uneven batches. Each job: an incident plane wave
+ * (incident = SIMK_JOB_PLANE_WAVE, ones) or a probe (SIMK_JOB_PROBE: aperture, aberrations and tilt from `probe`, its
+ * energy replaced by the job's) at (x, y) [A] through its own potential at its own energy; `intensity` (host,
+ * nx x ny float64 of that potential's grid) receives |exit wave|^2 after the last slice. Jobs of one grid shape advance
+ * together, one row and one column launch per slice step over the jobs still running; with SIMK_FORM_PLAIN they run
+ * one after another through the plain path (the sequential baseline). done_ms (optional, n_jobs) receives each job's
+ * completion time on the device from the start of the call. A potential may serve several jobs of one energy. */
+#define SIMK_JOB_PLANE_WAVE 0
+#define SIMK_JOB_PROBE 1
+typedef struct {
+    simk_potential* potential;
+    double energy;        /* [eV] */
+    int32_t incident;     /* SIMK_JOB_PLANE_WAVE or SIMK_JOB_PROBE */
+    int32_t reserved;
+    simk_probe probe;     /* probe jobs */
+    double x, y;          /* probe jobs: position [A] */
+    double* intensity;    /* out (host): nx x ny */
+} simk_job;
+int simk_job_table_run(simk_context* ctx, int32_t n_jobs, const simk_job* jobs, double* done_ms);
+
 /* ---- no-allocation variant ---------------------------------------------------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot let the library allocate device memory
  * (a host framework that owns all device memory through its own allocator, such as PyTorch's caching allocator or an

@@ -10,6 +10,7 @@ from .core import Antialias, AtomicStructure, ElectronBeam, Grid, Waves  # noqa:
 from .detector import (STEM, AnnularDetector, BinnedPixelatedDetector, CenterOfMassDetector,  # noqa: F401
                        PixelatedDetector, ScanMeasurement, SegmentedDetector, detector_shape)
 from .engine import Engine, ExecutionOptions  # noqa: F401
-from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, LobatoParameterization,  # noqa: F401
-                         Multislice, Potential, ProjectedPotential, Slicing, Surrogate, finite_profile)
+from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, JobTable,  # noqa: F401
+                         LobatoParameterization, Multislice, Potential, ProjectedPotential, Slicing, Surrogate,
+                         finite_profile)
 from .probe import Aberrations, Aperture, GridScan, Probe  # noqa: F401

@@ -32,7 +32,7 @@ EXPORTED = [
     "simk_run_batch", "simk_probe_spectrum", "simk_build_probes", "simk_detector_shape", "simk_scan",
     "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc", "simk_finite_profile",
     "simk_potential_from_atoms_finite", "simk_surrogate_train", "simk_surrogate_destroy", "simk_surrogate_info",
-    "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients",
+    "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients", "simk_job_table_run",
 ]
 SURROGATE_PARAMS = 11249
 
@@ -70,6 +70,14 @@ class Detector_t(C.Structure):
     _fields_ = [("kind", C.c_int32), ("max_angle", C.c_int32), ("units", C.c_int32), ("has_outer", C.c_int32),
                 ("nr", C.c_int32), ("nphi", C.c_int32), ("inner", C.c_double), ("outer", C.c_double),
                 ("rotation", C.c_double)]
+
+
+JOB_PLANE_WAVE, JOB_PROBE = 0, 1
+
+
+class Job_t(C.Structure):
+    _fields_ = [("potential", C.c_void_p), ("energy", C.c_double), ("incident", C.c_int32), ("reserved", C.c_int32),
+                ("probe", Probe_t), ("x", C.c_double), ("y", C.c_double), ("intensity", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -117,6 +125,7 @@ def _signatures(lib):
         "simk_surrogate_evaluate": [P, P, i32, PI32, PD, PD, PD, PD],
         "simk_surrogate_parameters": [P, P, C.POINTER(C.c_float), C.POINTER(C.c_float), PD],
         "simk_surrogate_gradients": [P, P, i32, PI32, PD, PD, PD, PD, C.POINTER(C.c_float), PD],
+        "simk_job_table_run": [P, i32, C.POINTER(Job_t), PD],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -463,6 +463,32 @@ int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_poten
     });
 }
 
+int simk_job_table_run(simk_context* ctx, int32_t n_jobs, const simk_job* jobs, double* done_ms) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx, "context is null");
+        SIMK_REQUIRE(n_jobs >= 0 && (n_jobs == 0 || jobs), "no job table");
+        std::vector<JobSpec> js(n_jobs);
+        for (int i = 0; i < n_jobs; ++i) {
+            const simk_job& j = jobs[i];
+            SIMK_REQUIRE(j.potential, "job " + std::to_string(i) + ": null potential");
+            SIMK_REQUIRE(j.incident == SIMK_JOB_PLANE_WAVE || j.incident == SIMK_JOB_PROBE,
+                         "job " + std::to_string(i) + ": unknown incident wave");
+            SIMK_REQUIRE(j.potential->impl.ctx == &ctx->impl,
+                         "job " + std::to_string(i) + ": the potential belongs to another context");
+            js[i].pot = &j.potential->impl;
+            js[i].energy = j.energy;
+            js[i].probe = (j.incident == SIMK_JOB_PROBE);
+            js[i].probe_spec = j.probe;
+            js[i].x = j.x;
+            js[i].y = j.y;
+            js[i].intensity = j.intensity;
+        }
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        run_job_table(ctx->impl, js, done_ms);
+    });
+}
+
 int simk_fft2(simk_context* ctx, int32_t nx, int32_t ny, int32_t count, int32_t inverse, int32_t precision,
               const double* in_re, const double* in_im, double* out_re, double* out_im) {
     return guarded([&] {

@@ -127,6 +127,11 @@ struct Context {
     int sm_count = 0;
     int64_t launches = 0;
     DeviceBuffer err_flag;  // int: set by a kernel whose bounded wait ran out
+    // Set by a job-table run for the duration of one slice step: wave b of the fused passes multiplies by the
+    // transmission slice wave_t[b] and by the propagator wave_p[b] among wave_p_blocks stacked ones (device arrays).
+    const float2* const* wave_t = nullptr;
+    const int* wave_p = nullptr;
+    int wave_p_blocks = 0;
     std::map<std::pair<int, int>, std::unique_ptr<LinePlan>> plans;
     std::map<std::tuple<int, int, double, double, double, double, double, double>, std::unique_ptr<Propagator>> props;
     // workspaces

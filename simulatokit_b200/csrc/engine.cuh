@@ -14,6 +14,22 @@ void run_waves(Context& ctx, PotentialImpl& pot, double energy, double tx, doubl
 void scan_device(Context& ctx, const simk_probe& probe, const std::vector<PotentialImpl*>& pots, int n_pos,
                  const double* positions_dev, int n_det, const simk_detector* dets, double* const* outputs_dev);
 
+void propagate_plain(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
+                     bool last_inverse, const std::function<void(int)>& on_slice);
+
+// One job of a job table: an incident plane wave (probe == false) or probe at (x, y) through `pot` at `energy`;
+// `intensity` (host, nx ny float64) receives |exit wave|^2.
+struct JobSpec {
+    PotentialImpl* pot = nullptr;
+    double energy = 0.0;
+    bool probe = false;
+    simk_probe probe_spec{};
+    double x = 0.0, y = 0.0;
+    double* intensity = nullptr;
+};
+// Every job of the table; done_ms[j] = device time from the start of the run to job j's exit intensity.
+void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_ms);
+
 // fused form (fused.cu)
 bool fused_supported(Context& ctx, const GridGeom& g);
 // Every slice on `count` waves in place. probe_rows_pending: the waves come from the probe's column IFFT and still

@@ -119,7 +119,7 @@ __device__ __forceinline__ void reg_fft(float2 (&v)[E], int t, const RegPlan& p,
 template <int E>
 __global__ void __launch_bounds__(rows_threads(E)) fused_rows_kernel(float2* __restrict__ psi, const float2* __restrict__ tmul,
                                                          RegPlan p, int nx, long long nrows, int inv, int fwd,
-                                                         float scale) {
+                                                         float scale, const float2* const* __restrict__ t_of_wave) {
     extern __shared__ __align__(16) float2 smem_rows[];
     const int t = threadIdx.x;
     const int rr = threadIdx.y;
@@ -134,9 +134,9 @@ __global__ void __launch_bounds__(rows_threads(E)) fused_rows_kernel(float2* __r
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = row[t + p.T * i];
     if (inv) reg_fft<E, +1>(v, t, p, sm);
-    if (tmul) {
+    if (tmul || t_of_wave) {
         const int ix = (int)(rc % nx);
-        const float2* tr = tmul + (long long)ix * ny;
+        const float2* tr = (t_of_wave ? t_of_wave[rc / nx] : tmul) + (long long)ix * ny;
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = cmul(v[i], __ldg(tr + t + p.T * i)) * scale;
     } else if (scale != 1.0f) {
@@ -162,7 +162,14 @@ struct ColArgs {
     const float2* spectrum;
     const float2* rx;
     const float2* ry;
+    const int* p_row;  // job tables: wave b uses the propagator P + p_row[b] N (null: every wave uses P)
+    int p_blocks;      // job tables: propagators stacked at P (for the tensor map)
 };
+
+// The propagator of wave b.
+__device__ __forceinline__ const float2* col_P(const ColArgs& a, long long b, long long N) {
+    return a.p_row ? a.P + (long long)a.p_row[b] * N : a.P;
+}
 
 template <int E>
 __global__ void __launch_bounds__(cols_threads(E)) fused_cols_kernel(ColArgs a, RegPlan p) {
@@ -188,8 +195,9 @@ __global__ void __launch_bounds__(cols_threads(E)) fused_cols_kernel(ColArgs a, 
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = col[(long long)(t + p.T * i) * ny];
         reg_fft<E, -1>(v, t, p, sm);
+        const float2* P = col_P(a, b, N);
 #pragma unroll
-        for (int i = 0; i < E; ++i) v[i] = cmul(v[i], __ldg(a.P + (long long)(t + p.T * i) * ny + iy)) * a.pscale;
+        for (int i = 0; i < E; ++i) v[i] = cmul(v[i], __ldg(P + (long long)(t + p.T * i) * ny + iy)) * a.pscale;
         if (a.mode == 0) reg_fft<E, +1>(v, t, p, sm);
     }
 #pragma unroll
@@ -288,7 +296,8 @@ __device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const Tw
 template <int N>
 __global__ void __launch_bounds__(256) fused_rows_ct(float2* __restrict__ psi, const float2* __restrict__ tmul,
                                                      const float2* __restrict__ tw, unsigned nx, unsigned nrows,
-                                                     int inv, int fwd, float scale) {
+                                                     int inv, int fwd, float scale,
+                                                     const float2* const* __restrict__ t_of_wave) {
     extern __shared__ __align__(16) float2 smem_rows_ct[];
     constexpr int T = N / 8;
     const unsigned t = threadIdx.x;
@@ -303,8 +312,8 @@ __global__ void __launch_bounds__(256) fused_rows_ct(float2* __restrict__ psi, c
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = row[t + T * i];
     if (inv) ct_fft_from<N, 0, +1>(v, t, tr, sm);
-    if (tmul) {
-        const float2* trow = tmul + (size_t)(rc % nx) * N;
+    if (tmul || t_of_wave) {
+        const float2* trow = (t_of_wave ? t_of_wave[rc / nx] : tmul) + (size_t)(rc % nx) * N;
 #pragma unroll
         for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], __ldg(trow + t + T * i)) * scale;
     } else if (scale != 1.0f) {
@@ -346,8 +355,9 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_ct(ColArgs a, const f
 #pragma unroll
         for (int i = 0; i < 8; ++i) v[i] = col[(size_t)(t + T * i) * ny];
         ct_fft_from<N, 0, -1>(v, t, tr, sm);
+        const float2* P = col_P(a, (long long)b, (long long)N * ny);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], __ldg(a.P + (size_t)(t + T * i) * ny + iy)) * a.pscale;
+        for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], __ldg(P + (size_t)(t + T * i) * ny + iy)) * a.pscale;
         if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, tr, sm);
     }
 #pragma unroll
@@ -399,7 +409,8 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     fused_cols_tma(const __grid_constant__ CUtensorMap map,
                                                                const __grid_constant__ CUtensorMap pmap,
                                                                float2* __restrict__ psi, float pscale, int ny,
-                                                               int count, const float2* __restrict__ tw, int* err) {
+                                                               int count, const float2* __restrict__ tw, int* err,
+                                                               const int* __restrict__ p_row) {
     extern __shared__ __align__(128) unsigned char smem_tma[];
     constexpr int T = N / 8;
     constexpr int BOXH = tma_box_rows(N);
@@ -428,11 +439,12 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
         float2* dst = stages + s * 2 * TILE;
+        const int prow = p_row ? p_row[b] * N : 0;  // job tables: this wave's propagator among the stacked ones
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
 #pragma unroll
         for (int k = 0; k < NBOX; ++k) {
             tma_load_2d(dst + k * BOXH * TC, &map, &full[s], 2 * iy0, b * N + k * BOXH);
-            tma_load_2d(dst + TILE + k * BOXH * TC, &pmap, &full[s], 2 * iy0, k * BOXH);
+            tma_load_2d(dst + TILE + k * BOXH * TC, &pmap, &full[s], 2 * iy0, prow + k * BOXH);
         }
     };
     unsigned tile = blockIdx.x;
@@ -502,7 +514,8 @@ template <int N, int RB, int ENG>
 __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)) fused_rows_tma(float2* __restrict__ psi,
                                                                const float2* __restrict__ tmul,
                                                                const float2* __restrict__ tw, int nx, int nrows,
-                                                               int inv, int fwd, float scale, int* err) {
+                                                               int inv, int fwd, float scale, int* err,
+                                                               const float2* const* __restrict__ t_of_wave) {
     extern __shared__ __align__(128) unsigned char smem_rtma[];
     constexpr int T = N / 8;
     constexpr int TILE = N * RB;
@@ -513,7 +526,7 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
     const int rr = threadIdx.y;
     const int tid = rr * T + (int)t;
     const int ntiles = nrows / RB;
-    const bool with_t = (tmul != nullptr);
+    const bool with_t = (tmul != nullptr) || (t_of_wave != nullptr);
     const uint32_t bytes = (uint32_t)(TILE * sizeof(float2));
     if (tid == 0) {
         mbar_init(&full[0], 1);
@@ -530,7 +543,10 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
         const int row0 = tile * RB;
         mbar_arrive_expect_tx(&full[s], with_t ? 2 * bytes : bytes);
         bulk_load(dst, psi + (size_t)row0 * N, bytes, &full[s]);
-        if (with_t) bulk_load(dst + TILE, tmul + (size_t)(row0 % nx) * N, bytes, &full[s]);
+        if (with_t) {
+            const float2* tb = t_of_wave ? t_of_wave[row0 / nx] : tmul;  // job tables: this wave's transmission
+            bulk_load(dst + TILE, tb + (size_t)(row0 % nx) * N, bytes, &full[s]);
+        }
     };
     int tile = blockIdx.x;
     if (tid == 0 && tile < ntiles) issue(tile, 0);
@@ -680,7 +696,8 @@ void launch_rows_e(Context& ctx, const RegPlan& p, float2* psi, const float2* tm
     }
     dim3 block(p.T, RB);
     const long long blocks = (nrows + RB - 1) / RB;
-    fused_rows_kernel<E><<<(unsigned)blocks, block, smem, ctx.stream>>>(psi, tmul, p, nx, nrows, inv, fwd, scale);
+    fused_rows_kernel<E><<<(unsigned)blocks, block, smem, ctx.stream>>>(psi, tmul, p, nx, nrows, inv, fwd, scale,
+                                                                        ctx.wave_t);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
 }
@@ -719,7 +736,7 @@ void launch_rows_ct(Context& ctx, const RegPlan& p, float2* psi, const float2* t
     dim3 block(T, RB);
     const long long blocks = (nrows + RB - 1) / RB;
     fused_rows_ct<N><<<(unsigned)blocks, block, smem, ctx.stream>>>(psi, tmul, p.tw, (unsigned)nx, (unsigned)nrows,
-                                                                    inv, fwd, scale);
+                                                                    inv, fwd, scale, ctx.wave_t);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
 }
@@ -770,7 +787,7 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     const long long ntiles = nrows / RB;
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(T, RB), smem, ctx.stream>>>(psi, tmul, p.tw, nx, (int)nrows, inv, fwd, scale,
-                                                  ctx.err_flag.as<int>());
+                                                  ctx.err_flag.as<int>(), ctx.wave_t);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
@@ -791,12 +808,13 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     if (blocks_per_sm <= 0) return false;
     ensure_err_flag(ctx);
     const CUtensorMap map = encode_tensor_map_2d(a.psi, 2ULL * a.ny, (unsigned long long)count * N, 2 * TC, BOXH);
-    const CUtensorMap pmap = encode_tensor_map_2d(const_cast<float2*>(a.P), 2ULL * a.ny, N, 2 * TC, BOXH);
+    const CUtensorMap pmap = encode_tensor_map_2d(const_cast<float2*>(a.P), 2ULL * a.ny,
+                                                  (unsigned long long)std::max(1, a.p_blocks) * N, 2 * TC, BOXH);
     const long long ntiles = (long long)count * (a.ny / TC);
     if (ntiles >= (1LL << 31)) return false;
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(TC, T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
-                                                  ctx.err_flag.as<int>());
+                                                  ctx.err_flag.as<int>(), a.p_row);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
@@ -995,7 +1013,12 @@ void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul
     }
 }
 
-void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a_in, int count) {
+    ColArgs a = a_in;
+    if (a.mode != 2 && ctx.wave_p) {  // job tables: per-wave propagators stacked at a.P
+        a.p_row = ctx.wave_p;
+        a.p_blocks = ctx.wave_p_blocks;
+    }
     const double bytes = (a.mode == 2 ? 8.0 : 16.0) * (double)p.n * a.ny * count;
     KernelTimer timer(ctx, "fused_cols", bytes);
     if (ctx.form == SIMK_FORM_BF16X3 && a.mode != 2) {  // the probe's inverse transform (mode 2) stays float32
@@ -1186,6 +1209,214 @@ void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe,
         KernelTimer t(ctx, "detect", 8.0 * (double)N * b);
         launch_detect(ctx, dplan, g, psi, b, first, outputs_dev, weight, 1.0f);
     }
+}
+
+// ---- job tables -------------------------------------------------------------------------------------------------------
+// Independent jobs (own grid, potential, energy, slice count; plane wave or probe) in the fewest launches: jobs of one
+// grid shape form a group whose waves sit side by side, sorted by slice count, so that at slice step s the jobs still
+// running are a prefix of the group. One row pass and one column pass per step advance that prefix, each wave reading
+// its own transmission slice and propagator through the context's wave table (wave_t, wave_p): the transmissions stay
+// in each potential's stack, the propagators are stacked once per group for the column pass's tensor map. The jobs
+// that end at step s complete their row inverse transform and write |exit wave|^2. With the plain form the jobs run
+// one after another through the plain path instead (the sequential baseline).
+namespace {
+__global__ void k_fill_c(float2* __restrict__ psi, long long n, float2 v) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        psi[i] = v;
+}
+__global__ void k_intensity(const float2* __restrict__ psi, long long n, double* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float2 v = psi[i];
+        out[i] = (double)v.x * v.x + (double)v.y * v.y;
+    }
+}
+int grid_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 16)); }
+
+// The incident wave of job j into psi (N float2): ones, or the probe IFFT(Psi0 r_x r_y) at (x, y).
+void incident_wave(Context& ctx, const JobSpec& j, float2* psi) {
+    const GridGeom& g = j.pot->g;
+    const long long N = g.count();
+    if (!j.probe) {
+        k_fill_c<<<grid_for(N), 256, 0, ctx.stream>>>(psi, N, make_float2(1.0f, 0.0f));
+        ++ctx.launches;
+        SIMK_CUDA(cudaGetLastError());
+        return;
+    }
+    simk_probe pr = j.probe_spec;
+    pr.energy = j.energy;
+    DeviceBuffer spectrum, pos(2 * sizeof(double)), rx(g.nx * sizeof(float2)), ry(g.ny * sizeof(float2));
+    probe_spectrum_device(ctx, g, pr, spectrum, nullptr);
+    const double xy[2] = {j.x, j.y};
+    SIMK_CUDA(cudaMemcpyAsync(pos.ptr, xy, sizeof(xy), cudaMemcpyHostToDevice, ctx.stream));
+    launch_ramps(ctx, g, pos.as<double>(), 0, 1, rx.as<float2>(), ry.as<float2>());
+    launch_probes(ctx, g, spectrum.as<float2>(), rx.as<float2>(), ry.as<float2>(), 1, psi, 1.0f);
+    fft2(ctx.plan(g.ny, 32), ctx.plan(g.nx, 32), psi, g.nx, g.ny, 1, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the temporaries above are freed on return
+}
+
+// Resets the context's wave table when a job run ends, also by an exception.
+struct WaveTableScope {
+    Context& c;
+    ~WaveTableScope() {
+        c.wave_t = nullptr;
+        c.wave_p = nullptr;
+        c.wave_p_blocks = 0;
+    }
+};
+}  // namespace
+
+void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_ms) {
+    const int n = (int)jobs.size();
+    if (n == 0) return;
+    std::map<const PotentialImpl*, double> energy_of;
+    for (int i = 0; i < n; ++i) {
+        const JobSpec& j = jobs[i];
+        SIMK_REQUIRE(j.pot && j.intensity, "job " + std::to_string(i) + ": null potential or output");
+        SIMK_REQUIRE(std::isfinite(j.energy) && j.energy > 0, "job " + std::to_string(i) + ": energy must be > 0");
+        SIMK_REQUIRE(!j.probe || (std::isfinite(j.x) && std::isfinite(j.y)), "job " + std::to_string(i) +
+                                                                               ": invalid probe position");
+        auto it = energy_of.find(j.pot);
+        SIMK_REQUIRE(it == energy_of.end() || it->second == j.energy,
+                     "job " + std::to_string(i) + ": a potential shared by jobs of different energies");
+        energy_of[j.pot] = j.energy;
+    }
+    for (auto& kv : energy_of) prepare_transmissions(ctx, *const_cast<PotentialImpl*>(kv.first), kv.second);
+    // the groups: jobs of one grid shape, longest first
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    for (int i = 0; i < n; ++i) groups[{jobs[i].pot->g.nx, jobs[i].pot->g.ny}].push_back(i);
+    for (auto& kv : groups)
+        std::stable_sort(kv.second.begin(), kv.second.end(), [&](int a, int b) {
+            return jobs[a].pot->n_slices() > jobs[b].pot->n_slices();
+        });
+    auto tilt = [&](const JobSpec& j, int k) {
+        return j.probe ? (k == 0 ? j.probe_spec.tilt_x : j.probe_spec.tilt_y) : 0.0;
+    };
+    cudaEvent_t start;
+    SIMK_CUDA(cudaEventCreate(&start));
+    std::vector<cudaEvent_t> events;
+    std::vector<std::pair<int, int>> event_jobs;  // (first, last) indices into `order` completed at each event
+    std::vector<int> order;
+    SIMK_CUDA(cudaEventRecord(start, ctx.stream));
+    WaveTableScope scope{ctx};
+    try {
+        for (auto& kv : groups) {
+            const std::vector<int>& ids = kv.second;
+            const int G = (int)ids.size();
+            const GridGeom& g0 = jobs[ids[0]].pot->g;
+            const long long N = g0.count();
+            const int nx = g0.nx, ny = g0.ny;
+            const int S = jobs[ids[0]].pot->n_slices();
+            DeviceBuffer waves((size_t)G * N * sizeof(float2)), inten((size_t)G * N * sizeof(double));
+            float2* psi = waves.as<float2>();
+            for (int w = 0; w < G; ++w) incident_wave(ctx, jobs[ids[w]], psi + (long long)w * N);
+            const int first_in_order = (int)order.size();
+            order.insert(order.end(), ids.begin(), ids.end());
+            if (ctx.form == SIMK_FORM_PLAIN) {
+                // the sequential baseline: each job alone through the plain path
+                for (int w = 0; w < G; ++w) {
+                    const JobSpec& j = jobs[ids[w]];
+                    propagate_plain(ctx, *j.pot, j.energy, tilt(j, 0), tilt(j, 1), psi + (long long)w * N, 1, true,
+                                    nullptr);
+                    k_intensity<<<grid_for(N), 256, 0, ctx.stream>>>(psi + (long long)w * N, N,
+                                                                      inten.as<double>() + (long long)w * N);
+                    ++ctx.launches;
+                    cudaEvent_t e;
+                    SIMK_CUDA(cudaEventCreate(&e));
+                    SIMK_CUDA(cudaEventRecord(e, ctx.stream));
+                    events.push_back(e);
+                    event_jobs.push_back({first_in_order + w, first_in_order + w + 1});
+                }
+                for (int w = 0; w < G; ++w)
+                    SIMK_CUDA(cudaMemcpyAsync(jobs[ids[w]].intensity, inten.as<double>() + (long long)w * N,
+                                              N * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+                SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+                continue;
+            }
+            // per step: each wave's transmission slice and propagator block
+            std::vector<const float2*> tptr((size_t)S * G, nullptr);
+            std::vector<int> prow((size_t)S * G, 0);
+            std::vector<const float2*> pblocks;
+            std::map<const float2*, int> block_of;
+            for (int w = 0; w < G; ++w) {
+                const JobSpec& j = jobs[ids[w]];
+                for (int s = 0; s < j.pot->n_slices(); ++s) {
+                    tptr[(size_t)s * G + w] = j.pot->t.as<float2>() + (long long)s * N;
+                    const float2* P = ctx.propagator(j.pot->g, j.energy, j.pot->dz[s], tilt(j, 0), tilt(j, 1))
+                                          .p.as<float2>();
+                    auto it = block_of.find(P);
+                    if (it == block_of.end()) {
+                        it = block_of.emplace(P, (int)pblocks.size()).first;
+                        pblocks.push_back(P);
+                    }
+                    prow[(size_t)s * G + w] = it->second;
+                }
+            }
+            DeviceBuffer pstack(pblocks.size() * N * sizeof(float2)), dt(tptr.size() * sizeof(float2*)),
+                dp(prow.size() * sizeof(int));
+            for (size_t b = 0; b < pblocks.size(); ++b)
+                SIMK_CUDA(cudaMemcpyAsync(pstack.as<float2>() + (long long)b * N, pblocks[b], N * sizeof(float2),
+                                          cudaMemcpyDeviceToDevice, ctx.stream));
+            SIMK_CUDA(cudaMemcpyAsync(dt.ptr, tptr.data(), tptr.size() * sizeof(float2*), cudaMemcpyHostToDevice,
+                                      ctx.stream));
+            SIMK_CUDA(cudaMemcpyAsync(dp.ptr, prow.data(), prow.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                      ctx.stream));
+            const RegPlan prw = reg_plan(ctx, ny);
+            const RegPlan pcl = reg_plan(ctx, nx);
+            auto active = [&](int s) {  // jobs with more than s slices: a prefix
+                int a = 0;
+                while (a < G && jobs[ids[a]].pot->n_slices() > s) ++a;
+                return a;
+            };
+            for (int s = 0; s < S; ++s) {
+                const int A = active(s);
+                ctx.wave_t = dt.as<const float2*>() + (size_t)s * G;
+                ctx.wave_p = dp.as<int>() + (size_t)s * G;
+                ctx.wave_p_blocks = (int)pblocks.size();
+                launch_rows(ctx, prw, psi, nullptr, nx, (long long)A * nx, s > 0 ? 1 : 0, 1, 1.0f);
+                ColArgs a{};
+                a.psi = psi;
+                a.P = pstack.as<float2>();
+                a.ny = ny;
+                a.mode = 0;
+                a.pscale = 1.0f / (float)N;
+                launch_cols(ctx, pcl, a, A);
+                ctx.wave_t = nullptr;
+                ctx.wave_p = nullptr;
+                ctx.wave_p_blocks = 0;
+                const int A1 = active(s + 1);
+                if (A1 == A) continue;
+                // jobs A1 .. A-1 have ended: complete their row inverse transform, intensities out
+                finish_rows(ctx, g0, psi + (long long)A1 * N, A - A1);
+                k_intensity<<<grid_for((long long)(A - A1) * N), 256, 0, ctx.stream>>>(
+                    psi + (long long)A1 * N, (long long)(A - A1) * N, inten.as<double>() + (long long)A1 * N);
+                ++ctx.launches;
+                cudaEvent_t e;
+                SIMK_CUDA(cudaEventCreate(&e));
+                SIMK_CUDA(cudaEventRecord(e, ctx.stream));
+                events.push_back(e);
+                event_jobs.push_back({first_in_order + A1, first_in_order + A});
+            }
+            for (int w = 0; w < G; ++w)
+                SIMK_CUDA(cudaMemcpyAsync(jobs[ids[w]].intensity, inten.as<double>() + (long long)w * N,
+                                          N * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+            SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the group's buffers are freed here
+        }
+        SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+        check_device_error(ctx);
+        for (size_t k = 0; k < events.size(); ++k) {
+            float ms = 0;
+            SIMK_CUDA(cudaEventElapsedTime(&ms, start, events[k]));
+            if (done_ms)
+                for (int q = event_jobs[k].first; q < event_jobs[k].second; ++q) done_ms[order[q]] = ms;
+        }
+    } catch (...) {
+        cudaStreamSynchronize(ctx.stream);
+        for (auto e : events) cudaEventDestroy(e);
+        cudaEventDestroy(start);
+        throw;
+    }
+    for (auto e : events) cudaEventDestroy(e);
+    cudaEventDestroy(start);
 }
 
 }  // namespace simk

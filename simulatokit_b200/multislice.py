@@ -416,6 +416,46 @@ class GaussianGenerator:
         return r * math.cos(theta)
 
 
+class JobTable:
+    """Independent multislice jobs, each its own potential, energy and incident wave (a plane wave or a probe at a
+    position), run as one table: jobs of one grid shape advance together, one row and one column launch per slice
+    step (simk_job_table_run). `run` returns each job's exit-wave intensity |psi|^2 (nx x ny) and its completion time
+    on the device [ms from the start of the call]. With ExecutionOptions(form="plain") the jobs run one after another
+    through the plain path: the sequential baseline."""
+
+    def __init__(self):
+        self.jobs = []
+
+    def add_plane_wave(self, potential: "Potential", energy: float):
+        self.jobs.append((potential, float(energy), None, None))
+        return self
+
+    def add_probe(self, potential: "Potential", probe, position):
+        self.jobs.append((potential, float(probe.beam.energy), probe, (float(position[0]), float(position[1]))))
+        return self
+
+    def run(self, options: ExecutionOptions | None = None, engine: Engine | None = None):
+        e = engine or Engine.require()
+        e.apply(options)
+        n = len(self.jobs)
+        outs = [np.zeros((p.grid.nx, p.grid.ny)) for p, _, _, _ in self.jobs]
+        arr = (L.Job_t * max(n, 1))()
+        for i, (p, energy, probe, pos) in enumerate(self.jobs):
+            h = p.handle(e).handle
+            arr[i].potential = h.value if isinstance(h, C.c_void_p) else h
+            arr[i].energy = energy
+            if probe is not None:
+                arr[i].incident = L.JOB_PROBE
+                arr[i].probe = probe.c()
+                arr[i].x, arr[i].y = pos
+            else:
+                arr[i].incident = L.JOB_PLANE_WAVE
+            arr[i].intensity = L.dptr(outs[i])
+        done = np.zeros(max(n, 1))
+        L.check(e.lib.simk_job_table_run(e.handle, n, arr, L.dptr(done)))
+        return outs, done[:n]
+
+
 class FrozenPhonons:
     """A frozen-phonon ensemble of one structure (FrozenPhonons.swift:61-156)."""
 
