@@ -431,6 +431,84 @@ def run_surrogate(args, sk, L, engine, stream, torch, local):
             "roofline": _roofline(kt, 1024), "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches}
 
 
+def random_jobs(n_jobs, seed):
+    """The uneven batch: per job a grid from {256, 384, 500, 640}^2, 10-200 slices of U(1, 2) A, an orthogonal cell
+    U(20, 40) A wide in x and y, U(80, 300) keV, a plane wave or a 20 mrad probe at the cell centre. Atoms fill the cell
+    at 0.08 A^-3 on a jittered lattice (spacing 0.08^(-1/3) = 2.32 A, jitter +-0.56 A per axis: minimum separation
+    1.2 A), each job's Z drawn uniformly from a palette of 3 elements drawn uniformly from 1-80."""
+    rng = np.random.default_rng(seed)
+    a = 0.08 ** (-1.0 / 3.0)
+    jit = 0.5 * (a - 1.2)
+    jobs = []
+    for _ in range(n_jobs):
+        n = int(rng.choice([256, 384, 500, 640]))
+        slices = int(rng.integers(10, 201))
+        dz = float(rng.uniform(1.0, 2.0))
+        lx, ly = rng.uniform(20.0, 40.0, 2)
+        box = (float(lx), float(ly), slices * dz)
+        nxl, nyl, nzl = (int(box[0] // a), int(box[1] // a), int(box[2] // a))
+        g = np.stack(np.meshgrid(np.arange(nxl), np.arange(nyl), np.arange(nzl), indexing="ij"), -1).reshape(-1, 3)
+        pos = (g + 0.5) * np.array([box[0] / nxl, box[1] / nyl, box[2] / nzl]) + rng.uniform(-jit, jit, g.shape)
+        palette = rng.choice(np.arange(1, 81), 3, replace=False)
+        nums = rng.choice(palette, len(pos))
+        energy = float(rng.uniform(80e3, 300e3))
+        probe = bool(rng.integers(0, 2))
+        jobs.append(dict(n=n, slices=slices, dz=dz, box=box, nums=nums, pos=pos, energy=energy, probe=probe))
+    return jobs
+
+
+def run_jobs(args, sk, L, engine, stream, torch, local):
+    """The uneven batch of 256 jobs: the job table (fused form, jobs of a grid shape advancing together) against the
+    same jobs run one after another in the plain form; potentials are built before the timed calls (all 256 jobs'
+    potentials and transmissions take about 70 GB of device memory; --jobs-chunk bounds it)."""
+    jobs = random_jobs(256, seed=1)
+    chunk = args.jobs_chunk
+    t_table, t_seq, done_table, dur_seq, steps = 0.0, 0.0, [], [], 0
+    for c0 in range(0, len(jobs), chunk):
+        part = jobs[c0:c0 + chunk]
+        table = sk.JobTable()
+        pots = []
+        for j in part:
+            st = sk.AtomicStructure(j["box"], j["nums"], j["pos"])
+            pot = sk.Potential(st, j["n"], j["n"], slice_thicknesses=[j["dz"]] * j["slices"])
+            pot.handle(engine)
+            pots.append(pot)
+            if j["probe"]:
+                pr = sk.Probe(sk.ElectronBeam(j["energy"]), pot.grid, sk.Aperture(20.0))
+                table.add_probe(pot, pr, (j["box"][0] / 2, j["box"][1] / 2))
+            else:
+                table.add_plane_wave(pot, j["energy"])
+            steps += j["slices"]
+        fused = sk.ExecutionOptions(form=args.form if args.form != "plain" else "fused")
+        table.run(options=fused, engine=engine)  # warm-up: transmissions, plans, propagators
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, done = table.run(options=fused, engine=engine)
+        t_table += time.perf_counter() - t0
+        done_table += list(done)
+        plain = sk.ExecutionOptions(form="plain")
+        table.run(options=plain, engine=engine)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, done_p = table.run(options=plain, engine=engine)
+        t_seq += time.perf_counter() - t0
+        dp = np.sort(done_p)
+        dur_seq += list(np.diff(np.concatenate([[0.0], dp])))
+        del pots, table
+    pct = lambda v, q: float(np.percentile(v, q))  # noqa: E731
+    return {"metric": "probe.slice steps/s", "value": steps / t_table, "ms_per_step": 1e3 * t_table,
+            "config": {"workload": "uneven batch: 256 jobs from seed 1, grids {256, 384, 500, 640}^2, 10-200 slices of "
+                                   "1-2 A, cells 20-40 A, 80-300 keV, plane wave or 20 mrad probe, exit-wave "
+                                   "intensities", "form": args.form, "steps": steps, "chunks_of": chunk},
+            "jobs": {"table_s": t_table, "sequential_plain_s": t_seq, "speedup": t_seq / t_table,
+                     "sequential_plain_steps_per_s": steps / t_seq,
+                     "table_completion_ms": {"p50": pct(done_table, 50), "p99": pct(done_table, 99)},
+                     "sequential_job_ms": {"p50": pct(dur_seq, 50), "p99": pct(dur_seq, 99)},
+                     "timing": "wall clock around each call (synchronising); completion times on the device from "
+                               "the start of the call; sequential job times = gaps between completions"},
+            "roofline": None, "cpu_baseline": None, "clocks": None, "gpu_launches": None}
+
+
 def run_extra(args):
     import torch
     import simulatokit_b200 as sk
@@ -444,7 +522,7 @@ def run_extra(args):
     torch.cuda.set_stream(stream)
     engine.set_stream(stream.cuda_stream)
     engine.apply(sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma))
-    fn = run_4dstem if args.workload == "4dstem" else run_surrogate
+    fn = {"4dstem": run_4dstem, "surrogate": run_surrogate, "jobs": run_jobs}[args.workload]
     line = fn(args, sk, L, engine, stream, torch, local)
     line.update({"unit": "probe.slice steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                  "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -470,10 +548,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
-    ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate"],
-                    help="stem: the headline STEM HAADF+BF scan; 4dstem and surrogate: the other scan configurations")
+    ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate", "jobs"],
+                    help="stem: the headline STEM HAADF+BF scan; 4dstem, surrogate, jobs: the other configurations")
     ap.add_argument("--sg-samples", type=int, default=10_000_000, help="surrogate workload: quadrature samples")
     ap.add_argument("--sg-steps", type=int, default=20000, help="surrogate workload: training steps")
+    ap.add_argument("--jobs-chunk", type=int, default=256, help="jobs workload: jobs per table call")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
