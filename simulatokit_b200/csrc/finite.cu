@@ -369,15 +369,20 @@ void build_potential_finite(Context& ctx, PotentialImpl& pot, int n_atoms, const
         DeviceBuffer did(in_dom.size() * sizeof(int)), dz(s.elements.size() * sizeof(int)),
             dpinf(s.elements.size() * nr * sizeof(double));
         std::vector<double> pinf(s.elements.size() * nr);
+        std::vector<float2> rf(s.elements.size() * nr);
         for (size_t e = 0; e < s.elements.size(); ++e)
-            for (int k = 0; k < nr; ++k)
-                pinf[e * nr + k] = infinite_profile(
-                    s.elements[e], s.rmin[e] * std::pow(s.rcut[e] / s.rmin[e], (double)k / (double)(nr - 1)));
+            for (int k = 0; k < nr; ++k) {
+                const double rho = s.rmin[e] * std::pow(s.rcut[e] / s.rmin[e], (double)k / (double)(nr - 1));
+                pinf[e * nr + k] = infinite_profile(s.elements[e], rho);
+                rf[e * nr + k] = make_float2((float)rho, (float)((std::log(rho) + 1.5) / 2.0));
+            }
+        DeviceBuffer drf(rf.size() * sizeof(float2));
+        SIMK_CUDA(cudaMemcpy(drf.ptr, rf.data(), rf.size() * sizeof(float2), cudaMemcpyHostToDevice));
         SIMK_CUDA(cudaMemcpy(did.ptr, in_dom.data(), in_dom.size() * sizeof(int), cudaMemcpyHostToDevice));
         SIMK_CUDA(cudaMemcpy(dz.ptr, s.elements.data(), s.elements.size() * sizeof(int), cudaMemcpyHostToDevice));
         SIMK_CUDA(cudaMemcpy(dpinf.ptr, pinf.data(), pinf.size() * sizeof(double), cudaMemcpyHostToDevice));
-        surrogate_profiles(ctx, *sg, d, did.as<int>(), (int)in_dom.size(), dz.as<int>(), dpinf.as<double>(), nr,
-                           table.as<double>());
+        surrogate_profiles(ctx, *sg, d, did.as<int>(), (int)in_dom.size(), dz.as<int>(), drf.as<float2>(),
+                           dpinf.as<double>(), nr, table.as<double>());
         SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
         // the quadrature judges a fixed sample of the surrogate's entries: up to 512 pairs x 8 radii
         const int npick = (int)std::min<size_t>(512, in_dom.size());

@@ -11,7 +11,7 @@
 // the trained domain, labelled by the float64 quadrature itself; each sample runs the network at both edges (rows b and
 // B + b of a doubled batch) and back-propagates +dF and -dF; mean-squared error; Adam. Every reduction runs in a fixed
 // order, so training is deterministic for a seed. Inference: tensor-core tiles of 16 queries per warp (k_sg_infer),
-// f16 weights and activations, float32 accumulation.
+// f16 weights and activations (SiLU in f16x2), float32 accumulation.
 //
 // Parameter layout (float32, kSurrogateParams values): emb[103][16] | W1[64][18] b1[64] | W2[64][64] b2[64] |
 // W3[64][64] b3[64] | W4[64] b4[1].
@@ -150,8 +150,7 @@ struct SgQueryPairs {  // queries from a profile table: pair p, radius k
     const int* pair_ids;      // the table rows this launch fills
     int npairs;
     const int* elem_z;        // Z of each element index of the potential
-    const double* rmin;
-    const double* rcut;
+    const float2* rho_f0;     // [element][nr]: the table's radius rho and the feature (log rho + 1.5) / 2
     const double* pinf;       // [element][nr]: P_inf at the table's radii
     int nr;
 };
@@ -175,6 +174,18 @@ __device__ __forceinline__ void mma_f16_16816(float (&d)[4], const uint32_t (&a)
 __device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
     const __half2 v = __floats2half2_rn(lo, hi);
     return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// SiLU of two accumulators as a packed f16 pair: silu(x) = x sigmoid(x) = h + h tanh(h) with h = x / 2, in f16x2 with
+// the hardware tanh approximation (one special-function operation per pair; the result is rounded to f16 for the
+// next layer in any case). The float32 SiLU of training needs an exponential and a reciprocal per value, which
+// made the activations, not the products, the inference's bottleneck.
+__device__ __forceinline__ uint32_t silu_f16x2(float a, float b) {
+    const __half2 h = __hmul2(__floats2half2_rn(a, b), __float2half2_rn(0.5f));
+    uint32_t t;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t*>(&h)));
+    const __half2 y = __hfma2(h, *reinterpret_cast<const __half2*>(&t), h);
+    return *reinterpret_cast<const uint32_t*>(&y);
 }
 
 // One hidden layer on 32 rows: acc = A (KS k-steps of 16) x W^T + bias, then SiLU into `out` as the next layer's A
@@ -207,8 +218,8 @@ __device__ __forceinline__ void tc_layer(const uint32_t (&a)[2][KS][4], const __
         // n-tile nt holds columns nt*8 .. nt*8+7: the first (nt even) or second half of the next layer's k-step nt/2
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
-            const uint32_t lo = pack_f16(silu(acc[mt][0]), silu(acc[mt][1]));
-            const uint32_t hi = pack_f16(silu(acc[mt][2]), silu(acc[mt][3]));
+            const uint32_t lo = silu_f16x2(acc[mt][0], acc[mt][1]);
+            const uint32_t hi = silu_f16x2(acc[mt][2], acc[mt][3]);
             out[mt][nt >> 1][(nt & 1) * 2] = lo;
             out[mt][nt >> 1][(nt & 1) * 2 + 1] = hi;
         }
@@ -257,31 +268,29 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_sg_infer(const float* __restr
         const long long qi = grp * 16 + (lane & 15);
         const bool valid = qi < total;
         int z = 1;
-        double rho = 1.0, zl = 0.0, zu = 1.0, pinf = 0.0;
+        double pinf = 0.0;
+        float f[2] = {0.0f, 0.0f};
         long long dst = 0;
         if (valid) {
             if (FROM_PAIRS) {
+                // the table's radius k of this element: its radius and first feature come from a per-build table,
+                // the edge feature asinh(z / rho) / 4 in float32 (it is rounded to f16 for the network anyway)
                 const int p = q.pair_ids[qi / q.nr], k = (int)(qi % q.nr);
                 const FinitePair pr = q.pairs[p];
                 z = q.elem_z[pr.elem];
-                const double r0 = q.rmin[pr.elem], r1 = q.rcut[pr.elem];
-                rho = r0 * pow(r1 / r0, (double)k / (double)(q.nr - 1));
-                zl = pr.zl;
-                zu = pr.zu;
+                const float2 rf = q.rho_f0[(size_t)pr.elem * q.nr + k];
+                f[0] = rf.y;
+                f[1] = 0.25f * asinhf((float)(lane < 16 ? pr.zu : pr.zl) / rf.x);
                 pinf = q.pinf[(size_t)pr.elem * q.nr + k];
                 dst = (long long)p * q.nr + k;
             } else {
                 z = qz[qi];
-                rho = qrho[qi];
-                zl = qzl[qi];
-                zu = qzu[qi];
+                surrogate_features(qrho[qi], lane < 16 ? qzu[qi] : qzl[qi], f);
                 pinf = qpinf[qi];
                 dst = qi;
             }
         }
         {
-            float f[2];
-            surrogate_features(rho, lane < 16 ? zu : zl, f);
             __half* row = x + lane * kTcLd1;
             const float* emb = params + OFF_EMB + (z - 1) * kEmbed;
 #pragma unroll
@@ -631,10 +640,11 @@ void surrogate_evaluate(Context& ctx, const SurrogateImpl& s, const std::vector<
 }
 
 void surrogate_profiles(Context& ctx, const SurrogateImpl& s, const FiniteDevice& d, const int* pair_ids_dev,
-                        int npairs, const int* elem_z_dev, const double* pinf_dev, int nr, double* table) {
+                        int npairs, const int* elem_z_dev, const float2* rho_f0_dev, const double* pinf_dev, int nr,
+                        double* table) {
     if (npairs == 0) return;
     set_infer_smem();
-    SgQueryPairs q{d.pairs, pair_ids_dev, npairs, elem_z_dev, d.rmin, d.rcut, pinf_dev, nr};
+    SgQueryPairs q{d.pairs, pair_ids_dev, npairs, elem_z_dev, rho_f0_dev, pinf_dev, nr};
     KernelTimer t(ctx, "surrogate_infer", 0.0);
     k_sg_infer<true><<<infer_blocks(ctx, (long long)npairs * nr), kTcWarps * 32, kTcSmem, ctx.stream>>>(
         s.params.as<float>(), q, nullptr, nullptr, nullptr, nullptr, nullptr, 0, table);

@@ -35,7 +35,8 @@ void surrogate_evaluate(Context& ctx, const SurrogateImpl& s, const std::vector<
 void surrogate_quadrature_points(Context& ctx, const std::vector<int>& z, const std::vector<double>& rho,
                                  const std::vector<double>& zl, const std::vector<double>& zu, double* out_dev);
 void surrogate_profiles(Context& ctx, const SurrogateImpl& s, const FiniteDevice& d, const int* pair_ids_dev,
-                        int npairs, const int* elem_z_dev, const double* pinf_dev, int nr, double* table);
+                        int npairs, const int* elem_z_dev, const float2* rho_f0_dev, const double* pinf_dev, int nr,
+                        double* table);
 double surrogate_gradients(Context& ctx, SurrogateImpl& s, const std::vector<int>& z, const std::vector<double>& rho,
                            const std::vector<double>& zl, const std::vector<double>& zu,
                            const std::vector<double>& target, float* grads_host);

@@ -110,9 +110,9 @@ def _f16(a):
 
 
 def test_tensor_core_inference_matches_oracle_network(engine, surrogate):
-    """The fused inference (f16 weights and activations on the tensor cores, float32 sums) against the oracle's
-    float64 network with the same f16 weights and inputs: what differs is the f16 rounding of the hidden activations
-    and the float32 sums."""
+    """The fused inference (f16 weights and activations on the tensor cores, float32 sums, SiLU in f16x2 through the
+    hardware tanh approximation) against the oracle's float64 network with the same f16 weights and inputs: what
+    differs is the f16 activations and their SiLU and the float32 sums."""
     flat, _ = surrogate.parameters()
     p = O.surrogate_unpack(flat)
     params = {k: (_f16(v) if k in ("emb", "W1", "W2", "W3") else v) for k, v in p.items()}
@@ -129,7 +129,8 @@ def test_tensor_core_inference_matches_oracle_network(engine, surrogate):
     err = np.abs(got / pinf - ref)
     rms, mx = float(np.sqrt(np.mean(err ** 2))), float(np.max(err))
     print(f"f16 tensor-core inference vs float64 network: rms {rms:.2e}, max {mx:.2e}")
-    assert rms <= 1e-3 and mx <= 5e-3, (rms, mx)
+    # the inference's own error must stay well below the network's fit (held-out rms |dF| about 5e-3): at most half
+    assert rms <= 2e-3 and mx <= 1e-2, (rms, mx)
 
 
 def test_trained_surrogate_is_judged_by_the_quadrature(engine, surrogate):
