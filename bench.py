@@ -521,7 +521,8 @@ def run_extra(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     engine.set_stream(stream.cuda_stream)
-    engine.apply(sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma))
+    engine.apply(sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma,
+                             autotune=args.autotune))
     fn = {"4dstem": run_4dstem, "surrogate": run_surrogate, "jobs": run_jobs}[args.workload]
     line = fn(args, sk, L, engine, stream, torch, local)
     line.update({"unit": "probe.slice steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -544,6 +545,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--col-tile", type=int, default=0)
     ap.add_argument("--no-tma", action="store_true")
+    ap.add_argument("--autotune", action="store_true", help="time column tile, TMA passes and batch on first use")
     ap.add_argument("--cpu-positions", type=int, default=32)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
@@ -582,7 +584,8 @@ def main():
     torch.cuda.set_stream(stream)
     assert stream.cuda_stream != 0
     engine.set_stream(stream.cuda_stream)
-    opts = sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma)
+    opts = sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma,
+                             autotune=args.autotune)
     engine.apply(opts)
 
     box, nums, pos = srtio3(8, 8, 20)
@@ -687,7 +690,8 @@ def main():
     forms, form_values = {}, {}
     if rank == 0 and world == 1 and not args.no_forms:
         for f in ("plain", "fused", "bf16x3"):
-            engine.apply(sk.ExecutionOptions(form=f, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma))
+            engine.apply(sk.ExecutionOptions(form=f, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma,
+                             autotune=args.autotune))
             engine.set_stream(stream.cuda_stream)
             scan_once()
             torch.cuda.synchronize()

@@ -150,6 +150,7 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                 c.col_tile = (int)value;
                 break;
             case SIMK_OPT_TMA: c.tma = value ? 1 : 0; break;
+            case SIMK_OPT_AUTOTUNE: c.autotune = value ? 1 : 0; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -190,6 +191,10 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_COL_TILE: *value = c.col_tile; break;
             case SIMK_OPT_TMA: *value = c.tma; break;
             case SIMK_OPT_GRAPHS_CACHED: *value = (int64_t)c.slice_graphs.size(); break;
+            case SIMK_OPT_AUTOTUNE: *value = c.autotune; break;
+            case SIMK_OPT_TUNED_COL_TILE: *value = c.last_tuned.col_tile; break;
+            case SIMK_OPT_TUNED_TMA: *value = c.last_tuned.tma; break;
+            case SIMK_OPT_TUNED_BATCH: *value = c.last_tuned.batch; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });

@@ -124,6 +124,13 @@ struct Context {
     int graphs = 1;
     int col_tile = 0;
     int tma = 1;            // TMA-pipelined persistent column pass where available
+    int autotune = 0;       // time the launch configurations on first use of a (grid, form)
+    struct Tuned {
+        int col_tile = -1, tma = -1;
+        long long batch = -1;
+    };
+    std::map<std::string, Tuned> tuned;
+    Tuned last_tuned;
     int sm_count = 0;
     int64_t launches = 0;
     DeviceBuffer err_flag;  // int: set by a kernel whose bounded wait ran out

@@ -168,6 +168,25 @@ void scan_device(Context& ctx, const simk_probe& probe, const std::vector<Potent
     const DeviceBuffer& spectrum = *sit->second;
     for (int d = 0; d < n_det; ++d)
         SIMK_CUDA(cudaMemsetAsync(outputs_dev[d], 0, (size_t)n_pos * dplan->det_count[d] * sizeof(double), ctx.stream));
+    // SIMK_OPT_AUTOTUNE: the tuned column tile, TMA choice and batch wherever the caller left them automatic, for
+    // this call only
+    struct Restore {
+        Context& c;
+        int tc, tma;
+        long long batch;
+        ~Restore() {
+            c.col_tile = tc;
+            c.tma = tma;
+            c.batch = batch;
+        }
+    } restore{ctx, ctx.col_tile, ctx.tma, ctx.batch};
+    if (ctx.autotune && ctx.form != SIMK_FORM_PLAIN && fused_supported(ctx, g)) {
+        prepare_transmissions(ctx, *pots[0], probe.energy);
+        const Context::Tuned t = autotune(ctx, *pots[0], probe.energy, probe.tilt_x, probe.tilt_y, n_pos);
+        if (ctx.col_tile == 0) ctx.col_tile = t.col_tile;
+        if (ctx.tma) ctx.tma = t.tma;
+        if (ctx.batch == 0) ctx.batch = t.batch;
+    }
     const long long B = batch_size(ctx, g, n_pos);
     ctx.work_a.ensure(B * N * sizeof(float2));
     ctx.rx.ensure(B * g.nx * sizeof(float2));

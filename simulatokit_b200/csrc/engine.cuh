@@ -30,6 +30,11 @@ struct JobSpec {
 // Every job of the table; done_ms[j] = device time from the start of the run to job j's exit intensity.
 void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_ms);
 
+// The launch configuration for fused scans of pot's grid with the context's form: the cached choice, or one made
+// by timing a slice step of pot's first transmission and propagator (SIMK_OPT_AUTOTUNE). The batch is chosen per grid
+// (up to 1024 waves within half the free memory), not per call; max_waves is unused.
+Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, long long max_waves);
+
 // fused form (fused.cu)
 bool fused_supported(Context& ctx, const GridGeom& g);
 // Every slice on `count` waves in place. probe_rows_pending: the waves come from the probe's column IFFT and still

@@ -1211,6 +1211,108 @@ void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe,
     }
 }
 
+// ---- autotuning ------------------------------------------------------------------------------------------------------
+// Candidates are timed on one slice step (row pass + column pass) of the potential's first transmission and
+// propagator over a scratch batch of waves (values do not change the time), with CUDA events after a warm-up: first
+// every (column tile, TMA) pair at a batch of up to 256 waves, then batch sizes from 32 waves up to what half of the
+// free device memory holds (the scan's wave buffer and its copy) for the winner. The figure of merit is time per
+// wave-step.
+Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, long long max_waves) {
+    const GridGeom& g = pot.g;
+    std::string key;
+    key_append(key, g.nx);
+    key_append(key, g.ny);
+    key_append(key, ctx.form);
+    auto it = ctx.tuned.find(key);
+    if (it != ctx.tuned.end()) {
+        ctx.last_tuned = it->second;
+        return it->second;
+    }
+    const long long N = g.count();
+    size_t free_b = 0, total_b = 0;
+    SIMK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    long long cap = (long long)(free_b / 2 / (2 * (size_t)N * sizeof(float2)));
+    cap = std::max(1LL, std::min(cap, 1024LL));  // per grid, not per call: the caller's batches cap themselves
+    (void)max_waves;
+    const RegPlan prw = reg_plan(ctx, g.ny);
+    const RegPlan pcl = reg_plan(ctx, g.nx);
+    const Propagator& P = ctx.propagator(g, energy, pot.dz[0], tx, ty);
+    DeviceBuffer buf((size_t)cap * N * sizeof(float2));
+    SIMK_CUDA(cudaMemsetAsync(buf.ptr, 0, (size_t)cap * N * sizeof(float2), ctx.stream));
+    const int save_tc = ctx.col_tile, save_tma = ctx.tma, save_timing = ctx.timing;
+    ctx.timing = 0;
+    cudaEvent_t e0, e1;
+    SIMK_CUDA(cudaEventCreate(&e0));
+    SIMK_CUDA(cudaEventCreate(&e1));
+    auto step = [&](long long b) {
+        launch_rows(ctx, prw, buf.as<float2>(), pot.t.as<float2>(), g.nx, b * g.nx, 1, 1, 1.0f);
+        ColArgs a{};
+        a.psi = buf.as<float2>();
+        a.P = P.p.as<float2>();
+        a.ny = g.ny;
+        a.mode = 0;
+        a.pscale = 1.0f / (float)N;
+        launch_cols(ctx, pcl, a, (int)b);
+    };
+    auto time_per_wave = [&](long long b) {
+        step(b);  // warm-up (first launches set attributes and occupancy)
+        SIMK_CUDA(cudaEventRecord(e0, ctx.stream));
+        for (int r = 0; r < 2; ++r) step(b);
+        SIMK_CUDA(cudaEventRecord(e1, ctx.stream));
+        SIMK_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        SIMK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return (double)ms / (2.0 * (double)b);
+    };
+    Context::Tuned best;
+    double best_t = 1e300;
+    try {
+        const long long b0 = std::min(cap, 256LL);
+        for (int tma : {1, 0}) {
+            if (tma && !save_tma) continue;
+            if (!tma && ctx.form == SIMK_FORM_BF16X3) continue;  // the tensor-core form runs on the TMA passes only
+            for (int tc : {2, 4, 8}) {
+                if (g.ny % tc || tc * (g.nx / 8) > 1024) continue;
+                ctx.tma = tma;
+                ctx.col_tile = tc;
+                const double t = time_per_wave(b0);
+                if (t < best_t) {
+                    best_t = t;
+                    best.col_tile = tc;
+                    best.tma = tma;
+                    best.batch = b0;
+                }
+            }
+        }
+        ctx.tma = best.tma;
+        ctx.col_tile = best.col_tile;
+        for (long long b = 32; b <= cap; b *= 2) {
+            if (b == best.batch) continue;
+            const double t = time_per_wave(b);
+            if (t < best_t * 0.98) {  // a larger batch must gain more than the noise
+                best_t = t;
+                best.batch = b;
+            }
+        }
+    } catch (...) {
+        ctx.col_tile = save_tc;
+        ctx.tma = save_tma;
+        ctx.timing = save_timing;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    ctx.col_tile = save_tc;
+    ctx.tma = save_tma;
+    ctx.timing = save_timing;
+    SIMK_CUDA(cudaEventDestroy(e0));
+    SIMK_CUDA(cudaEventDestroy(e1));
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the scratch batch is freed on return
+    ctx.tuned[key] = best;
+    ctx.last_tuned = best;
+    return best;
+}
+
 // ---- job tables -------------------------------------------------------------------------------------------------------
 // Independent jobs (own grid, potential, energy, slice count; plane wave or probe) in the fewest launches: jobs of one
 // grid shape form a group whose waves sit side by side, sorted by slice count, so that at slice step s the jobs still

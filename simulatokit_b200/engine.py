@@ -18,12 +18,14 @@ class ExecutionOptions:
     form: "plain" (one operation per launch), "fused" (batched fused passes, the default) or "bf16x3" (fused with
     tensor-core DFT stages). batch: waves per batch (0 = from batch_bytes). batch_bytes: bytes of waves one batch
     may hold (default 1 GiB). graphs: capture each batch's slice loop in a CUDA graph. col_tile: columns per CTA of
-    the fused column pass (0 = automatic). tma: the TMA-pipelined persistent column pass where available."""
+    the fused column pass (0 = automatic). tma: the TMA-pipelined persistent column pass where available. autotune:
+    time the column tile, TMA passes and batch size on the first fused scan of a grid and use the fastest where the
+    settings above are automatic."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
     def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
-                 col_tile: int = 0, tma: bool = True):
+                 col_tile: int = 0, tma: bool = True, autotune: bool = False):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
         self.form = form
@@ -32,6 +34,7 @@ class ExecutionOptions:
         self.graphs = bool(graphs)
         self.col_tile = int(col_tile)
         self.tma = bool(tma)
+        self.autotune = bool(autotune)
 
     @staticmethod
     def standard() -> "ExecutionOptions":
@@ -75,6 +78,7 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_GRAPHS, 1 if o.graphs else 0))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COL_TILE, o.col_tile))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TMA, 1 if o.tma else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_AUTOTUNE, 1 if o.autotune else 0))
 
     def set_stream(self, stream_ptr: int | None):
         L.check(self.lib.simk_context_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
@@ -86,6 +90,15 @@ class Engine:
         v = C.c_int64(0)
         L.check(self.lib.simk_context_launch_count(self.handle, C.byref(v), 1 if reset else 0))
         return int(v.value)
+
+    def tuned(self) -> dict:
+        """The last autotuning's choice (-1 before any): column tile, TMA passes, batch."""
+        out = {}
+        for k, opt in (("col_tile", L.OPT_TUNED_COL_TILE), ("tma", L.OPT_TUNED_TMA), ("batch", L.OPT_TUNED_BATCH)):
+            v = C.c_int64(0)
+            L.check(self.lib.simk_context_get_option(self.handle, opt, C.byref(v)))
+            out[k] = int(v.value)
+        return out
 
     def graphs_cached(self) -> int:
         """Slice loops the context holds as instantiated CUDA graphs."""
