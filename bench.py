@@ -727,7 +727,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "form": args.form, "batch": args.batch, "col_tile": args.col_tile,
-                           "tma": not args.no_tma,
+                           "tma": not args.no_tma, "autotune": args.autotune,
                            "positions": n_pos, "slices": 20,
                            "grid": [NX, NY], "replicas": world, "l2": "inputs larger than L2 (batch of waves up to "
                                                                      "1 GiB per launch)"},

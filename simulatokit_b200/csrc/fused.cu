@@ -1216,7 +1216,7 @@ void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe,
 // propagator over a scratch batch of waves (values do not change the time), with CUDA events after a warm-up: first
 // every (column tile, TMA) pair at a batch of up to 256 waves, then batch sizes from 32 waves up to what half of the
 // free device memory holds (the scan's wave buffer and its copy) for the winner. The figure of merit is time per
-// wave-step.
+// wave-step; of the batches, the largest within 2 % of the fastest is kept.
 Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, long long max_waves) {
     const GridGeom& g = pot.g;
     std::string key;
@@ -1286,14 +1286,17 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
         }
         ctx.tma = best.tma;
         ctx.col_tile = best.col_tile;
-        for (long long b = 32; b <= cap; b *= 2) {
-            if (b == best.batch) continue;
-            const double t = time_per_wave(b);
-            if (t < best_t * 0.98) {  // a larger batch must gain more than the noise
-                best_t = t;
-                best.batch = b;
-            }
-        }
+        // batch: the largest whose time per wave is within 2 % of the fastest, since the per-batch work that is not
+        // timed here (probe generation, detection, launches) favours large batches
+        std::vector<std::pair<long long, double>> bt{{best.batch, best_t}};
+        for (long long b = 32; b <= cap; b *= 2)
+            if (b != best.batch) bt.push_back({b, time_per_wave(b)});
+        double fastest = 1e300;
+        for (auto& x : bt) fastest = std::min(fastest, x.second);
+        for (auto& x : bt)
+            if (x.second <= 1.02 * fastest && x.first > best.batch) best.batch = x.first;
+        for (auto& x : bt)
+            if (x.first == best.batch) best_t = x.second;
     } catch (...) {
         ctx.col_tile = save_tc;
         ctx.tma = save_tma;
