@@ -224,6 +224,15 @@ int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_poten
                      simk_potential* const* potentials, int32_t n_positions, const double* positions_xy_device,
                      int32_t n_detectors, const simk_detector* detectors, double* const* outputs_device);
 
+/* STEM.scan(probe:potentials:scan:detector:) with a WavesDetector (Sources/SimulatoDetector/WavesDetector.swift:115-137,
+ * collect :191-216): the complex exit wave at every position through one potential, resampled in Fourier space to
+ * rows x columns points over the same extent (Waves.resampled, Sources/SimulatoCore/WavesResample.swift:16-43:
+ * the lowest frequencies kept, or all of them zero-padded, values' amplitude kept); rows = columns = 0 keeps the
+ * simulation grid. out_re / out_im: host, n_positions x rows x columns float64, positions in the given order.
+ * STEM.scanFrozenPhonons with a WavesDetector is this call once per configuration. */
+int simk_scan_waves(simk_context* ctx, const simk_probe* probe, simk_potential* potential, int32_t n_positions,
+                    const double* positions_xy, int32_t rows, int32_t columns, double* out_re, double* out_im);
+
 /* ---- job tables ----------------------------------------------------------------------------------------------------
  * No reference counterpart as one call (the reference runs such jobs one Multislice.run at a time, Multislice.swift:52-80
  * -> MetalEngine.swift:458-474); proposed as simk_job_table_run for uneven batches. Each job: an incident plane wave

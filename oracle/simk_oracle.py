@@ -696,6 +696,47 @@ def stem_scan(probe: ProbeSpec, potentials, positions, detectors, thicknesses_li
 
 
 # ---------------------------------------------------------------------------------------------------------------------
+# Waves detector (Sources/SimulatoDetector/WavesDetector.swift:35-216, Sources/SimulatoCore/WavesResample.swift:16-55)
+# ---------------------------------------------------------------------------------------------------------------------
+
+def resample_map(n: int, m: int):
+    """Waves.resampleMap (WavesResample.swift:46-54): (source, destination) of every frequency kept going from n to m
+    points: the lowest m (crop, crop_indices order) or all n (zero-pad, positive frequencies first)."""
+    if m <= n:
+        if m == 1:
+            return [(0, 0)]
+        return [(int(src), dst) for dst, src in enumerate(crop_indices(n, m))]
+    if n == 1:
+        return [(0, 0)]
+    positive = n // 2 if n % 2 == 0 else n // 2 + 1
+    return [(i, i if i < positive else m - n + i) for i in range(n)]
+
+
+def resample_wave(psi: np.ndarray, rows: int, columns: int) -> np.ndarray:
+    """Waves.resampled (WavesResample.swift:16-43): FFT, keep the mapped frequencies on the rows x columns grid, inverse
+    FFT, times rows columns / (nx ny) so that the values keep their amplitude."""
+    nx, ny = psi.shape
+    f = np.fft.fft2(psi)
+    out = np.zeros((rows, columns), dtype=np.complex128)
+    mx, my = resample_map(nx, rows), resample_map(ny, columns)
+    sx, dx = [a for a, _ in mx], [b for _, b in mx]
+    sy, dy = [a for a, _ in my], [b for _, b in my]
+    out[np.ix_(dx, dy)] = f[np.ix_(sx, sy)]
+    return np.fft.ifft2(out) * (rows * columns / (nx * ny))
+
+
+def waves_scan(probe: "ProbeSpec", g: Grid, vs, thicknesses, positions, gpts=None) -> np.ndarray:
+    """STEM.scan with a WavesDetector (WavesDetector.swift:115-126, collect :191-216): the exit wave at every position
+    through one potential, resampled to gpts = (rows, columns) when given; [position][row][column]."""
+    ts = [transmission(v, probe.energy, g) for v in vs]
+    out = []
+    for pos in positions:
+        ex = multislice(build_probe(probe, g, pos), ts, thicknesses, probe.energy, g, tilt=probe.tilt)[-1]
+        out.append(ex if gpts is None else resample_wave(ex, gpts[0], gpts[1]))
+    return np.array(out)
+
+
+# ---------------------------------------------------------------------------------------------------------------------
 # Frozen phonons (Sources/SimulatoMultislice/FrozenPhonons.swift:14-156)
 # ---------------------------------------------------------------------------------------------------------------------
 _M64 = (1 << 64) - 1

@@ -8,7 +8,8 @@ every compute call raises CudaUnavailable."""
 from ._lib import CudaFailure, CudaUnavailable, InvalidArgument, SimulatoError  # noqa: F401
 from .core import Antialias, AtomicStructure, ElectronBeam, Grid, Waves  # noqa: F401
 from .detector import (STEM, AnnularDetector, BinnedPixelatedDetector, CenterOfMassDetector,  # noqa: F401
-                       PixelatedDetector, ScanMeasurement, SegmentedDetector, detector_shape)
+                       PixelatedDetector, ScanMeasurement, ScanWaves, SegmentedDetector, WavesDetector,
+                       detector_shape)
 from .engine import Engine, ExecutionOptions  # noqa: F401
 from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, JobTable,  # noqa: F401
                          LobatoParameterization, Multislice, Potential, ProjectedPotential, Slicing, Surrogate,

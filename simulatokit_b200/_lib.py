@@ -34,6 +34,7 @@ EXPORTED = [
     "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc", "simk_finite_profile",
     "simk_potential_from_atoms_finite", "simk_surrogate_train", "simk_surrogate_destroy", "simk_surrogate_info",
     "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients", "simk_job_table_run",
+    "simk_scan_waves",
 ]
 SURROGATE_PARAMS = 11249
 
@@ -127,6 +128,7 @@ def _signatures(lib):
         "simk_surrogate_parameters": [P, P, C.POINTER(C.c_float), C.POINTER(C.c_float), PD],
         "simk_surrogate_gradients": [P, P, i32, PI32, PD, PD, PD, PD, C.POINTER(C.c_float), PD],
         "simk_job_table_run": [P, i32, C.POINTER(Job_t), PD],
+        "simk_scan_waves": [P, C.POINTER(Probe_t), P, i32, PD, i32, i32, PD, PD],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

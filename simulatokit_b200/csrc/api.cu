@@ -468,6 +468,22 @@ int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_poten
     });
 }
 
+int simk_scan_waves(simk_context* ctx, const simk_probe* probe, simk_potential* potential, int32_t n_positions,
+                    const double* positions_xy, int32_t rows, int32_t columns, double* out_re, double* out_im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && probe && potential, "null argument");
+        SIMK_REQUIRE(n_positions >= 1 && positions_xy && out_re && out_im, "no scan position or output");
+        SIMK_REQUIRE((rows == 0 && columns == 0) || (rows >= 2 && columns >= 2),
+                     "the waves detector needs at least 2 points per axis (or 0, 0 for the simulation grid)");
+        for (int i = 0; i < 2 * n_positions; ++i)
+            SIMK_REQUIRE(std::isfinite(positions_xy[i]), "invalid position " + std::to_string(i / 2));
+        SIMK_REQUIRE(potential->impl.ctx == &ctx->impl, "the potential belongs to another context");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        scan_waves(ctx->impl, *probe, potential->impl, n_positions, positions_xy, rows, columns, out_re, out_im);
+    });
+}
+
 int simk_job_table_run(simk_context* ctx, int32_t n_jobs, const simk_job* jobs, double* done_ms) {
     return guarded([&] {
         SIMK_REQUIRE(ctx, "context is null");

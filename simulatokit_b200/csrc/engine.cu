@@ -208,4 +208,110 @@ void scan_device(Context& ctx, const simk_probe& probe, const std::vector<Potent
     }
 }
 
+// ---- the waves detector --------------------------------------------------------------------------------------------
+// Waves.resampled (WavesResample.swift:16-43) on the device: the exit spectrum FFT2(exit) is at hand after the last
+// slice (the fused form stops there for the detectors; the plain form too, times 1/N), so resampling is a gather of
+// the frequencies kept (Waves.resampleMap: the lowest rows x columns, or all of them zero-padded) into the target
+// spectrum followed by one inverse transform of the target size; rows columns / N (abTEM's scaling) times the
+// inverse's 1 / (rows columns) leaves 1 / N, applied in the gather. Without resampling the map is the identity.
+namespace {
+__global__ void k_resample_gather(const float2* __restrict__ S, long long N, int ny, const int* __restrict__ srcx,
+                                  const int* __restrict__ srcy, int rows, int cols, int count, float scale,
+                                  float2* __restrict__ out) {
+    const long long M = (long long)rows * cols;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M * count;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long w = i / M, o = i - w * M;
+        const int dx = (int)(o / cols), dy = (int)(o - (long long)dx * cols);
+        const int sx = srcx[dx], sy = srcy[dy];
+        out[i] = (sx >= 0 && sy >= 0) ? S[w * N + (long long)sx * ny + sy] * scale : make_float2(0.0f, 0.0f);
+    }
+}
+
+// For every destination index of an axis resampled from n to m points, its source frequency or -1 (zero padding).
+std::vector<int> resample_sources(int n, int m) {
+    std::vector<int> src(m, -1);
+    if (m <= n) {
+        if (m == 1) {
+            src[0] = 0;
+            return src;
+        }
+        // the first m/2 (even m) or floor(m/2) + 1 (odd m) frequencies, then the last floor(m/2)
+        const int low = (m % 2) ? m / 2 + 1 : m / 2, high = m / 2;
+        for (int d = 0; d < low; ++d) src[d] = d;
+        for (int d = 0; d < high; ++d) src[low + d] = n - high + d;
+        return src;
+    }
+    if (n == 1) {
+        src[0] = 0;
+        return src;
+    }
+    const int positive = (n % 2 == 0) ? n / 2 : n / 2 + 1;
+    for (int i = 0; i < n; ++i) src[i < positive ? i : m - n + i] = i;
+    return src;
+}
+}  // namespace
+
+void scan_waves(Context& ctx, const simk_probe& probe, PotentialImpl& pot, int n_pos, const double* positions_xy,
+                int rows, int columns, double* out_re, double* out_im) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    if (rows == 0 && columns == 0) {
+        rows = g.nx;
+        columns = g.ny;
+    }
+    SIMK_REQUIRE(rows >= 2 && columns >= 2, "the waves detector needs at least 2 points per axis");
+    const long long M = (long long)rows * columns;
+    prepare_transmissions(ctx, pot, probe.energy);
+    DeviceBuffer spectrum, pos((size_t)2 * n_pos * sizeof(double));
+    probe_spectrum_device(ctx, g, probe, spectrum, nullptr);
+    SIMK_CUDA(cudaMemcpyAsync(pos.ptr, positions_xy, (size_t)2 * n_pos * sizeof(double), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    const std::vector<int> sx = resample_sources(g.nx, rows), sy = resample_sources(g.ny, columns);
+    DeviceBuffer dsx(sx.size() * sizeof(int)), dsy(sy.size() * sizeof(int));
+    SIMK_CUDA(cudaMemcpyAsync(dsx.ptr, sx.data(), sx.size() * sizeof(int), cudaMemcpyHostToDevice, ctx.stream));
+    SIMK_CUDA(cudaMemcpyAsync(dsy.ptr, sy.data(), sy.size() * sizeof(int), cudaMemcpyHostToDevice, ctx.stream));
+    const long long B = batch_size(ctx, g, n_pos);
+    ctx.work_a.ensure(B * N * sizeof(float2));
+    ctx.rx.ensure(B * g.nx * sizeof(float2));
+    ctx.ry.ensure(B * g.ny * sizeof(float2));
+    const bool fused = (ctx.form != SIMK_FORM_PLAIN) && fused_supported(ctx, g);
+    if (fused) ctx.work_b.ensure(B * N * sizeof(float2));
+    DeviceBuffer outb((size_t)B * M * sizeof(float2));
+    std::vector<float2> h((size_t)B * M);
+    const LinePlan& prow = ctx.plan(g.ny, 32);
+    const LinePlan& pcol = ctx.plan(g.nx, 32);
+    for (long long first = 0; first < n_pos; first += B) {
+        const int b = (int)std::min<long long>(B, n_pos - first);
+        float2* psi = ctx.work_a.as<float2>();
+        float scale;
+        if (fused) {
+            exit_spectra_fused(ctx, pot, probe, spectrum.as<float2>(), pos.as<double>(), first, b);
+            scale = 1.0f / (float)N;
+        } else {
+            launch_ramps(ctx, g, pos.as<double>(), first, b, ctx.rx.as<float2>(), ctx.ry.as<float2>());
+            launch_probes(ctx, g, spectrum.as<float2>(), ctx.rx.as<float2>(), ctx.ry.as<float2>(), b, psi, 1.0f);
+            fft2_timed(ctx, prow, pcol, psi, g.nx, g.ny, b, +1, 1.0 / (double)N);
+            propagate_plain(ctx, pot, probe.energy, probe.tilt_x, probe.tilt_y, psi, b, false, nullptr);
+            scale = 1.0f;  // the last slice already carries the 1 / N of the transform it skipped
+        }
+        const long long total = M * b;
+        k_resample_gather<<<(int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16)), 256, 0,
+                            ctx.stream>>>(psi, N, g.ny, dsx.as<int>(), dsy.as<int>(), rows, columns, b, scale,
+                                          outb.as<float2>());
+        SIMK_CUDA(cudaGetLastError());
+        ++ctx.launches;
+        fft2(ctx.plan(columns, 32), ctx.plan(rows, 32), outb.ptr, rows, columns, b, +1, 1.0, ctx.stream,
+             &ctx.launches);
+        SIMK_CUDA(cudaMemcpyAsync(h.data(), outb.ptr, (size_t)total * sizeof(float2), cudaMemcpyDeviceToHost,
+                                  ctx.stream));
+        SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+        for (long long i = 0; i < total; ++i) {
+            out_re[first * M + i] = h[i].x;
+            out_im[first * M + i] = h[i].y;
+        }
+    }
+    check_device_error(ctx);
+}
+
 }  // namespace simk

@@ -43,6 +43,13 @@ bool fused_supported(Context& ctx, const GridGeom& g);
 void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
                      bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last);
 void finish_rows(Context& ctx, const GridGeom& g, float2* psi, int count);
+// The probes of positions [first, first + b) through every slice, left as FFT2(exit wave) in ctx.work_a.
+void exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                        const double* positions_dev, long long first, int b);
+// STEM.scan with a WavesDetector: the exit wave at every position (host positions), resampled in Fourier space to
+// rows x columns points (0, 0: the simulation grid), into host float64 arrays [position][row][column].
+void scan_waves(Context& ctx, const simk_probe& probe, PotentialImpl& pot, int n_pos, const double* positions_xy,
+                int rows, int columns, double* out_re, double* out_im);
 void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
                       const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
                       double* const* outputs_dev, double weight);

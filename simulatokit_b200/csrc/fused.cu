@@ -1187,11 +1187,9 @@ void finish_rows(Context& ctx, const GridGeom& g, float2* psi, int count) {
     launch_rows(ctx, prow, psi, nullptr, g.nx, (long long)count * g.nx, 1, 0, 1.0f);
 }
 
-void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
-                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
-                      double* const* outputs_dev, double weight) {
+void exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                        const double* positions_dev, long long first, int b) {
     const GridGeom& g = pot.g;
-    const long long N = g.count();
     float2* psi = ctx.work_a.as<float2>();
     launch_ramps(ctx, g, positions_dev, first, b, ctx.rx.as<float2>(), ctx.ry.as<float2>());
     const RegPlan pcol = reg_plan(ctx, g.nx);
@@ -1205,9 +1203,17 @@ void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe,
     a.pscale = 1.0f;
     launch_cols(ctx, pcol, a, b);
     propagate_fused(ctx, pot, probe.energy, probe.tilt_x, probe.tilt_y, psi, b, true, nullptr, true);
+}
+
+void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
+                      double* const* outputs_dev, double weight) {
+    const GridGeom& g = pot.g;
+    const long long N = g.count();
+    exit_spectra_fused(ctx, pot, probe, spectrum, positions_dev, first, b);
     {
         KernelTimer t(ctx, "detect", 8.0 * (double)N * b);
-        launch_detect(ctx, dplan, g, psi, b, first, outputs_dev, weight, 1.0f);
+        launch_detect(ctx, dplan, g, ctx.work_a.as<float2>(), b, first, outputs_dev, weight, 1.0f);
     }
 }
 

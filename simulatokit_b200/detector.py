@@ -7,12 +7,13 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import _lib as L
-from .core import Grid, _refuse
+from .core import Grid, Waves, _refuse
 from .engine import Engine, ExecutionOptions
 from .multislice import Backend
 
@@ -93,6 +94,76 @@ class BinnedPixelatedDetector:
         return L.Detector_t(L.DET_BINNED, 0, 0, 1, self.gpts[0], self.gpts[1], 0.0, self.max_angle, 0.0)
 
 
+class WavesDetector:
+    """The complex exit wave at every position (abTEM's WavesDetector; WavesDetector.swift:35-67): on the simulation grid,
+    or resampled in Fourier space to rows x columns points over the same extent (Waves.resampled,
+    WavesResample.swift:16-43)."""
+
+    def __init__(self, rows: int | None = None, columns: int | None = None):
+        if (rows is None) != (columns is None):
+            _refuse("give both rows and columns, or neither")
+        for n in (rows, columns):
+            if n is not None and not (isinstance(n, (int, np.integer)) and n >= 2):
+                _refuse(f"unsupported grid length {n}")
+        self.rows, self.columns = rows, columns
+
+    @staticmethod
+    def required_bytes(positions: int, rows: int, columns: int) -> int:
+        """complex float64 waves: 16 bytes a point (WavesDetector.requiredBytes)."""
+        return positions * rows * columns * 16
+
+
+def _physical_memory_half() -> int:
+    try:
+        return os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") // 2
+    except (ValueError, OSError, AttributeError):
+        return 1 << 62
+
+
+@dataclass
+class ScanWaves:
+    """The exit waves of a scan (ScanWaves, WavesDetector.swift:71-106): values[position][row][column], positions
+    row-major over (scan x, scan y), on `grid` (the detector's rows x columns over the simulation extent)."""
+    scan_shape: list
+    grid: Grid
+    beam: object
+    values: np.ndarray
+
+    def __getitem__(self, ix_iy) -> Waves:
+        ix, iy = ix_iy
+        return Waves(self.values[ix * self.scan_shape[1] + iy], self.grid, self.beam, "reciprocal_space")
+
+    def array(self) -> np.ndarray:
+        return self.values.reshape(tuple(self.scan_shape) + (self.grid.nx, self.grid.ny))
+
+
+def _waves_scan(probe, potential, scan, detector: WavesDetector, engine: Engine) -> ScanWaves:
+    rows = detector.rows or probe.grid.nx
+    columns = detector.columns or probe.grid.ny
+    positions = np.ascontiguousarray(scan.positions, dtype=np.float64)
+    n = len(positions)
+    re = np.zeros(n * rows * columns)
+    im = np.zeros(n * rows * columns)
+    p = probe.c()
+    h = potential.handle(engine).handle
+    L.check(engine.lib.simk_scan_waves(engine.handle, C.byref(p), h, n, L.dptr(positions), detector.rows or 0,
+                                       detector.columns or 0, L.dptr(re), L.dptr(im)))
+    grid = Grid(rows, columns, probe.grid.extent_x, probe.grid.extent_y)
+    return ScanWaves(list(scan.shape), grid, probe.beam, (re + 1j * im).reshape(n, rows, columns))
+
+
+def _check_waves_memory(probe, scan, detector: WavesDetector, configurations: int, limit: int | None):
+    rows = detector.rows or probe.grid.nx
+    columns = detector.columns or probe.grid.ny
+    positions = len(scan.positions) * configurations
+    need = WavesDetector.required_bytes(positions, rows, columns)
+    limit = _physical_memory_half() if limit is None else limit
+    if need > limit:
+        _refuse(f"{positions} exit waves of {rows} x {columns} points need {need} bytes, more than the {limit} bytes "
+                f"allowed (half of the physical memory); scan fewer positions or configurations, or detect on a "
+                f"smaller rows x columns")
+
+
 def detector_shape(detector, grid: Grid, energy: float):
     g = grid.c()
     d = detector.c()
@@ -124,7 +195,21 @@ class STEM:
 
     @staticmethod
     def scan(probe, potentials, scan, detectors, backend: Backend = Backend.cuda,
-             options: ExecutionOptions | None = None, engine: Engine | None = None):
+             options: ExecutionOptions | None = None, engine: Engine | None = None, memory_limit: int | None = None):
+        """`detectors`: a list of measurement detectors (-> one ScanMeasurement each, averaged over the potentials), or
+        a WavesDetector (-> ScanWaves of the single potential; memory_limit defaults to half the physical memory)."""
+        if isinstance(detectors, WavesDetector):
+            # STEM.scan(probe:potentials:scan:detector: WavesDetector) (WavesDetector.swift:115-137): one potential
+            if len(potentials) != 1:
+                _refuse(f"the waves detector takes one potential, got {len(potentials)}"
+                        + ("" if not potentials else ": averaging complex waves over configurations is not "
+                           "meaningful; scan the configurations with STEM.scanFrozenPhonons"))
+            if not potentials[0].grid.matches(probe.grid):
+                _refuse("grid mismatch")
+            _check_waves_memory(probe, scan, detectors, 1, memory_limit)
+            e = engine or Engine.require()
+            e.apply(options)
+            return _waves_scan(probe, potentials[0], scan, detectors, e)
         if not potentials:
             _refuse("no potential")
         for p in potentials:
@@ -150,7 +235,16 @@ class STEM:
 
     @staticmethod
     def scanFrozenPhonons(probe, phonons, nx, ny, slice_thickness, scan, detectors, parameterization=None,
-                          options: ExecutionOptions | None = None, engine: Engine | None = None):
-        """The scan averaged over every configuration of a FrozenPhonons ensemble."""
+                          options: ExecutionOptions | None = None, engine: Engine | None = None,
+                          memory_limit: int | None = None):
+        """The scan averaged over every configuration of a FrozenPhonons ensemble; with a WavesDetector, one ScanWaves
+        per configuration instead (complex waves are not averaged, WavesDetector.swift:141-173)."""
         pots = phonons.lazy_potentials(nx, ny, slice_thickness, parameterization)
+        if isinstance(detectors, WavesDetector):
+            if not pots:
+                _refuse("no potential")
+            _check_waves_memory(probe, scan, detectors, len(pots), memory_limit)
+            e = engine or Engine.require()
+            e.apply(options)
+            return [_waves_scan(probe, p, scan, detectors, e) for p in pots]
         return STEM.scan(probe, pots, scan, detectors, options=options, engine=engine)

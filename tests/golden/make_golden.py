@@ -29,7 +29,7 @@ KEEP = {
     "slice-2": None,   # all (1.4 MB)
     "slice-4": None,
     "slice-4-scan": ["com_mrad", "com_inv", "dp"],
-    "waves": ["full"],
+    "waves": None,     # all six runs (1.5 MB): full size and five Fourier resamplings
 }
 
 

@@ -125,3 +125,22 @@ def test_beam_matches_pins():
         b = sk.ElectronBeam(row["energy"])
         assert b.wavelength == row["wavelength"]
         assert abs(b.interaction_parameter - row["sigma"]) <= 1e-15 * row["sigma"]
+
+
+def test_waves_detector_refusals_on_the_host():
+    """WavesDetector(rows:columns:) and STEM.scan's waves refusals (WavesDetector.swift:41-48, 115-131) need no device."""
+    import simulatokit_b200 as sk
+    from oracle import simk_oracle as O
+    with pytest.raises(sk.InvalidArgument):
+        sk.WavesDetector(1, 8)
+    with pytest.raises(sk.InvalidArgument):
+        sk.WavesDetector(8, None)
+    s = O.al_fcc_cell()
+    st = sk.AtomicStructure(s.box, s.numbers, s.positions)
+    pots = [sk.Potential(st, 48, 48, slice_thickness=2.025) for _ in range(2)]
+    probe = sk.Probe(sk.ElectronBeam(200e3), pots[0].grid, sk.Aperture(20.0))
+    scan = sk.GridScan((0.0, 0.0), (4.05, 4.05), 3, 2)
+    with pytest.raises(sk.InvalidArgument, match="one potential, got 2"):
+        sk.STEM.scan(probe, pots, scan, sk.WavesDetector())
+    with pytest.raises(sk.InvalidArgument, match="one potential, got 0"):
+        sk.STEM.scan(probe, [], scan, sk.WavesDetector())

@@ -253,3 +253,38 @@ def test_gaussian_generator_statistics():
     b = O.frozen_displacements([14] * 10, {14: 0.075}, 2, 1)
     assert np.array_equal(a[0], b[0]) and not np.array_equal(a[0], a[1])
     assert O.configuration_seed(1, 0) != O.configuration_seed(0, 1)
+
+
+def _waves_setup():
+    w = G.pins()["waves"]
+    s = O.Structure(tuple(w["box"]), np.array([a[0] for a in w["atoms"]], dtype=int),
+                    np.array([a[1] for a in w["atoms"]], dtype=np.float64))
+    n = w["gpts"]
+    op = O.Potential.from_structure(s, n, n, slice_thickness=w["sliceThickness"], pi_choice="abtem")
+    positions = O.grid_scan_positions(w["scan"]["start"], w["scan"]["end"], *w["scan"]["gpts"])
+    return w, op, positions
+
+
+@pytest.mark.parametrize("run", range(6))
+def test_waves_detector_runs(run):
+    """WavesDetectorTests.exitWavesMatchAbTEM (Detector/WavesDetectorTests.swift): the exit waves of a 3 x 2 scan, full
+    size and Fourier-resampled (crop and zero-pad, odd and even sizes), at assert_allclose's float64 defaults (rtol
+    1e-7, atol 1e-12 of the wave maximum)."""
+    w, op, positions = _waves_setup()
+    entry = w["runs"][run]
+    got = O.waves_scan(O.ProbeSpec(w["energy"], w["semiangle"]), op.grid, op.build(), op.thicknesses, positions,
+                       entry["gpts"])
+    ref = G.array("waves", entry["name"])
+    got = got.reshape(ref.shape)
+    atol = 1e-12 * np.max(np.abs(ref))
+    for a, b in ((got.real, ref.real), (got.imag, ref.imag)):
+        assert np.all(np.abs(a - b) <= atol + 1e-7 * np.abs(b)), entry["name"]
+
+
+def test_resample_map_round_trip():
+    """Cropping after zero-padding returns the original frequencies (WavesResampleTests)."""
+    rng = np.random.default_rng(3)
+    psi = rng.standard_normal((12, 9)) + 1j * rng.standard_normal((12, 9))
+    up = O.resample_wave(psi, 25, 16)
+    back = O.resample_wave(up, 12, 9)
+    assert np.max(np.abs(back - psi)) <= 1e-12 * np.max(np.abs(psi))
