@@ -329,11 +329,11 @@ def run_4dstem(args, sk, L, engine, stream, torch, local):
     a = 5.431
     box, nums, pos = silicon(6, 6, 20)
     st = sk.AtomicStructure(box, nums, pos)
-    fp = sk.FrozenPhonons(st, sigmas={14: 0.075}, configurations=16, seed=1)
+    fp = sk.FrozenPhonons(st, sigmas={14: 0.075}, configurations=args.configs, seed=1)
     pots = [sk.Potential(fp.configuration(c), 768, 768, slice_thickness=1.35775) for c in range(fp.count)]
     assert pots[0].slice_count == 80
     probe = sk.Probe(sk.ElectronBeam(300e3), pots[0].grid, sk.Aperture(25.0), sk.Aberrations(C10=-50.0))
-    scan = sk.GridScan((3 * a, 3 * a), (4 * a, 4 * a), 48, 48)
+    scan = sk.GridScan((3 * a, 3 * a), (4 * a, 4 * a), args.scan, args.scan)
     dets = [sk.BinnedPixelatedDetector(60.0, (128, 128)), sk.CenterOfMassDetector("valid", "mrad")]
     positions = np.asarray(scan.positions)
     run, outs = _device_scan(sk, L, engine, probe, pots, positions, dets, torch)
@@ -361,9 +361,10 @@ def run_4dstem(args, sk, L, engine, stream, torch, local):
         errs = {"binned": float(np.linalg.norm(o1[0].cpu().numpy() - ref[0].ravel()) / np.linalg.norm(ref[0])),
                 "com": float(np.linalg.norm(o1[1].cpu().numpy() - ref[1].ravel()) / np.linalg.norm(ref[1]))}
     return {"metric": "probe.slice steps/s", "value": value, "ms_per_step": ms / args.steps,
-            "config": {"workload": "4D-STEM with frozen phonons, Si 6x6x20 (5760 atoms, 108.6 A), 768x768, 80 slices "
-                                   "of 1.35775 A, 16 configurations (sigma 0.075 A, seed 1), 300 keV, 25 mrad, "
-                                   "C10 = -50 A, 48x48 scan over one unit cell, binned 128x128 up to 60 mrad + COM",
+            "config": {"workload": f"4D-STEM with frozen phonons, Si 6x6x20 (5760 atoms, 108.6 A), 768x768, 80 "
+                                   f"slices of 1.35775 A, {args.configs} configurations (sigma 0.075 A, seed 1), "
+                                   f"300 keV, 25 mrad, C10 = -50 A, {args.scan}x{args.scan} scan over one unit cell, "
+                                   "binned 128x128 up to 60 mrad + COM",
                        "form": args.form, "steps_per_scan": steps},
             "roofline": _roofline(kt, 768), "cpu_baseline": cpu, "rel_l2_vs_fp64": errs, "clocks": clocks,
             "gpu_launches": launches}
@@ -555,6 +556,8 @@ def main():
     ap.add_argument("--sg-samples", type=int, default=10_000_000, help="surrogate workload: quadrature samples")
     ap.add_argument("--sg-steps", type=int, default=20000, help="surrogate workload: training steps")
     ap.add_argument("--jobs-chunk", type=int, default=256, help="jobs workload: jobs per table call")
+    ap.add_argument("--configs", type=int, default=16, help="4dstem workload: frozen-phonon configurations")
+    ap.add_argument("--scan", type=int, default=48, help="4dstem workload: scan positions per side")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

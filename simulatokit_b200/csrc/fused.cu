@@ -401,7 +401,8 @@ template <int N, int ENG>
 using EngineState = std::conditional_t<ENG == 0, TwRegs<N>, std::conditional_t<ENG == 1, Dft16Frags, int>>;
 
 // Blocks per SM the tensor-core engine asks the compiler for: two when a block has at most 256 threads (at most 128
-// registers a thread), else one.
+// registers a thread), else one. (Asking the float32 shared-memory engine for more blocks by capping it at 84
+// registers made it spill and lose 12 % at 768^2: it keeps the compiler's choice.)
 constexpr int tc_min_blocks(int threads, int eng) { return (eng == 1 && threads <= 256) ? 2 : 1; }
 
 template <int N, int TC, int MODE, int ENG>
