@@ -400,10 +400,15 @@ constexpr int rows_per_tile(int n) {
 template <int N, int ENG>
 using EngineState = std::conditional_t<ENG == 0, TwRegs<N>, std::conditional_t<ENG == 1, Dft16Frags, int>>;
 
-// Blocks per SM the tensor-core engine asks the compiler for: two when a block has at most 256 threads (at most 128
-// registers a thread), else one. (Asking the float32 shared-memory engine for more blocks by capping it at 84
-// registers made it spill and lose 12 % at 768^2: it keeps the compiler's choice.)
-constexpr int tc_min_blocks(int threads, int eng) { return (eng == 1 && threads <= 256) ? 2 : 1; }
+// Blocks per SM the engines ask the compiler for. The tensor-core engine: two when a block has at most 256 threads
+// (at most 128 registers a thread). The float32 register engine: three for its 256-thread blocks (at most 85
+// registers; 512^2 fits without spills and gains a third block per SM). The float32 shared-memory engine keeps the
+// compiler's choice (capped at 84 registers it spilled and lost 12 % at 768^2).
+constexpr int tc_min_blocks(int threads, int eng) {
+    if (eng == 1) return threads <= 256 ? 2 : 1;
+    if (eng == 0) return threads == 256 ? 3 : 1;
+    return 1;
+}
 
 template <int N, int TC, int MODE, int ENG>
 __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG))
