@@ -233,6 +233,25 @@ int simk_scan_device(simk_context* ctx, const simk_probe* probe, int32_t n_poten
 int simk_scan_waves(simk_context* ctx, const simk_probe* probe, simk_potential* potential, int32_t n_positions,
                     const double* positions_xy, int32_t rows, int32_t columns, double* out_re, double* out_im);
 
+/* ---- contrast transfer function (Sources/SimulatoProbe/ContrastTransferFunction.swift) -----------------------------
+ * An objective lens: aberrations (the simk_probe order), aperture semiangle [mrad] (INFINITY: none) with abTEM's soft
+ * edge when `soft`, focal spread Delta [A] (temporal envelope) and angular spread beta [mrad] (spatial envelope). */
+typedef struct {
+    double aberrations[25];
+    double semiangle_mrad;
+    int32_t soft;
+    int32_t reserved;
+    double focal_spread;
+    double angular_spread;
+} simk_ctf;
+/* ContrastTransferFunction.kernel (ContrastTransferFunction.swift:85-115), float64 on the device, FFT order. */
+int simk_ctf_kernel(simk_context* ctx, const simk_grid* grid, double energy, const simk_ctf* ctf, double* re,
+                    double* im);
+/* Waves.applying (ContrastTransferFunction.swift:146-161) on `count` waves: IFFT(FFT(psi) H) in float32 with the
+ * float64-computed kernel; out_re / out_im (the waves) and out_intensity (|.|^2, the HRTEM image) are optional (NULL). */
+int simk_apply_ctf(simk_context* ctx, const simk_grid* grid, double energy, const simk_ctf* ctf, int32_t count,
+                   const double* in_re, const double* in_im, double* out_re, double* out_im, double* out_intensity);
+
 /* ---- job tables ----------------------------------------------------------------------------------------------------
  * No reference counterpart as one call (the reference runs such jobs one Multislice.run at a time, Multislice.swift:52-80
  * -> MetalEngine.swift:458-474); proposed as simk_job_table_run for uneven batches. Each job: an incident plane wave

@@ -442,6 +442,92 @@ def aperture_values(g: Grid, lam: float, semiangle_mrad: float, soft: bool = Tru
     return out
 
 
+def _ab(ab: dict, k: str) -> float:
+    return float(ab.get(k, 0.0))
+
+
+def dchi_dalpha(alpha, phi, ab: dict, lam: float):
+    """Aberrations.dChiDAlpha (ContrastTransferFunction.swift:12-21): abTEM's d chi / d alpha."""
+    g = lambda k: _ab(ab, k)  # noqa: E731
+    p, a = phi, alpha
+    t1 = (g("C12") * np.cos(2 * (p - g("phi12"))) + g("C10")) * a
+    t2 = (g("C23") * np.cos(3 * (p - g("phi23"))) + g("C21") * np.cos(1 * (p - g("phi21")))) * a ** 2
+    t3 = (g("C34") * np.cos(4 * (p - g("phi34"))) + g("C32") * np.cos(2 * (p - g("phi32"))) + g("C30")) * a ** 3
+    t4 = (g("C45") * np.cos(5 * (p - g("phi45"))) + g("C43") * np.cos(3 * (p - g("phi43")))
+          + g("C41") * np.cos(1 * (p - g("phi41")))) * a ** 4
+    t5 = (g("C56") * np.cos(6 * (p - g("phi56"))) + g("C54") * np.cos(4 * (p - g("phi54")))
+          + g("C52") * np.cos(2 * (p - g("phi52"))) + g("C50")) * a ** 5
+    return 2 * math.pi / lam * (t1 + t2 + t3 + t4 + t5)
+
+
+def dchi_dphi(alpha, phi, ab: dict, lam: float):
+    """Aberrations.dChiDPhi (ContrastTransferFunction.swift:24-34): abTEM's azimuthal term."""
+    g = lambda k: _ab(ab, k)  # noqa: E731
+    p, a = phi, alpha
+    t1 = 1 / 2.0 * (2.0 * g("C12") * np.sin(2.0 * (p - g("phi12")))) * a
+    t2 = 1 / 3.0 * (3.0 * g("C23") * np.sin(3.0 * (p - g("phi23"))) + 1.0 * g("C21") * np.sin(1.0 * (p - g("phi21")))) * a ** 2
+    t3 = 1 / 4.0 * (4.0 * g("C34") * np.sin(4.0 * (p - g("phi34"))) + 2.0 * g("C32") * np.sin(2.0 * (p - g("phi32")))) * a ** 3
+    t4 = 1 / 5.0 * (5.0 * g("C45") * np.sin(5.0 * (p - g("phi45"))) + 3.0 * g("C43") * np.sin(3.0 * (p - g("phi43")))
+                    + 1.0 * g("C41") * np.sin(1.0 * (p - g("phi41")))) * a ** 4
+    t5 = (1 / 6.0) * (6.0 * g("C56") * np.sin(6.0 * (p - g("phi56"))) + 4.0 * g("C54") * np.sin(4.0 * (p - g("phi54")))
+                      + 2.0 * g("C52") * np.sin(2.0 * (p - g("phi52")))) * a ** 5
+    return -2 * math.pi / lam * (t1 + t2 + t3 + t4 + t5)
+
+
+def temporal_envelope(alpha, lam: float, focal_spread: float):
+    """exp(-((pi/2 / lambda) Delta alpha^2)^2) (ContrastTransferFunction.swift:68-72)."""
+    x = 0.5 * math.pi / lam * focal_spread * alpha * alpha
+    return np.exp(-(x * x))
+
+
+def spatial_envelope(alpha, phi, lam: float, ab: dict, angular_spread: float):
+    """exp(-sign(beta) (beta/2)^2 ((d chi/d alpha)^2 + (d chi/d phi)^2)), beta in mrad (:75-82)."""
+    b = angular_spread / 1e3
+    dk = dchi_dalpha(alpha, phi, ab, lam)
+    dp = dchi_dphi(alpha, phi, ab, lam)
+    sign = 1.0 if b > 0 else (-1.0 if b < 0 else 0.0)
+    return np.exp(-sign * (b / 2) * (b / 2) * (dk * dk + dp * dp))
+
+
+def ctf_kernel(g: "Grid", energy: float, ab: dict, cutoff_mrad: float = math.inf, soft: bool = True,
+               focal_spread: float = 0.0, angular_spread: float = 0.0) -> np.ndarray:
+    """ContrastTransferFunction.kernel (:85-115): exp(-i chi) x E_s (beta != 0) x E_t (Delta != 0) x aperture (finite
+    cutoff), FFT order."""
+    lam = wavelength(energy)
+    kx, ky = g.kx()[:, None], g.ky()[None, :]
+    alpha = np.sqrt(kx * kx + ky * ky) * lam
+    phi = np.arctan2(ky + 0 * kx, kx + 0 * ky)
+    h = np.exp(-1j * chi(alpha, phi, ab, lam))
+    if angular_spread != 0:
+        h = h * spatial_envelope(alpha, phi, lam, ab, angular_spread)
+    if focal_spread != 0:
+        h = h * temporal_envelope(alpha, lam, focal_spread)
+    if math.isfinite(cutoff_mrad):
+        h = h * aperture_values(g, lam, cutoff_mrad, soft)
+    return h
+
+
+def apply_ctf(psi: np.ndarray, kernel: np.ndarray) -> np.ndarray:
+    """Waves.applying (ContrastTransferFunction.swift:146-161): IFFT(FFT(psi) H)."""
+    return np.fft.ifft2(np.fft.fft2(psi) * kernel)
+
+
+def scherzer_defocus(cs: float, energy: float, factor: float = 1.5) -> float:
+    """sign(Cs) sqrt(factor |Cs| lambda) (:118-124)."""
+    s = 1.0 if cs > 0 else (-1.0 if cs < 0 else 0.0)
+    return s * math.sqrt(factor * abs(cs) * wavelength(energy))
+
+
+def point_resolution(cs: float, energy: float, divisor: float = 6.0) -> float:
+    """(lambda^3 |Cs| / divisor)^(1/4) (:127-131)."""
+    return math.pow(math.pow(wavelength(energy), 3) * abs(cs) / divisor, 1.0 / 4)
+
+
+def nyquist_sampling(semiangle: float, energy: float, oversampling: float = 4.0) -> float:
+    """1 / (oversampling alpha_c / lambda 1e-3) (:134-142)."""
+    return 1 / (oversampling * semiangle / wavelength(energy) * 1e-3)
+
+
 @dataclass
 class ProbeSpec:
     energy: float

@@ -14,4 +14,4 @@ from .engine import Engine, ExecutionOptions  # noqa: F401
 from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, JobTable,  # noqa: F401
                          LobatoParameterization, Multislice, Potential, ProjectedPotential, Slicing, Surrogate,
                          finite_profile)
-from .probe import Aberrations, Aperture, GridScan, Probe  # noqa: F401
+from .probe import Aberrations, Aperture, ContrastTransferFunction, GridScan, Probe  # noqa: F401

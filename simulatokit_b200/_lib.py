@@ -34,7 +34,7 @@ EXPORTED = [
     "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc", "simk_finite_profile",
     "simk_potential_from_atoms_finite", "simk_surrogate_train", "simk_surrogate_destroy", "simk_surrogate_info",
     "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients", "simk_job_table_run",
-    "simk_scan_waves",
+    "simk_scan_waves", "simk_ctf_kernel", "simk_apply_ctf",
 ]
 SURROGATE_PARAMS = 11249
 
@@ -72,6 +72,11 @@ class Detector_t(C.Structure):
     _fields_ = [("kind", C.c_int32), ("max_angle", C.c_int32), ("units", C.c_int32), ("has_outer", C.c_int32),
                 ("nr", C.c_int32), ("nphi", C.c_int32), ("inner", C.c_double), ("outer", C.c_double),
                 ("rotation", C.c_double)]
+
+
+class Ctf_t(C.Structure):
+    _fields_ = [("aberrations", C.c_double * 25), ("semiangle_mrad", C.c_double), ("soft", C.c_int32),
+                ("reserved", C.c_int32), ("focal_spread", C.c_double), ("angular_spread", C.c_double)]
 
 
 JOB_PLANE_WAVE, JOB_PROBE = 0, 1
@@ -129,6 +134,8 @@ def _signatures(lib):
         "simk_surrogate_gradients": [P, P, i32, PI32, PD, PD, PD, PD, C.POINTER(C.c_float), PD],
         "simk_job_table_run": [P, i32, C.POINTER(Job_t), PD],
         "simk_scan_waves": [P, C.POINTER(Probe_t), P, i32, PD, i32, i32, PD, PD],
+        "simk_ctf_kernel": [P, C.POINTER(Grid_t), d, C.POINTER(Ctf_t), PD, PD],
+        "simk_apply_ctf": [P, C.POINTER(Grid_t), d, C.POINTER(Ctf_t), i32, PD, PD, PD, PD, PD],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

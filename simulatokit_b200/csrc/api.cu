@@ -293,6 +293,7 @@ int simk_potential_read_transmission(simk_context* ctx, simk_potential* potentia
         prepare_transmissions(ctx->impl, potential->impl, energy);
         const long long N = potential->impl.g.count();
         std::vector<float2> h(N);
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));  // the copy below is not ordered after that stream
         SIMK_CUDA(cudaMemcpy(h.data(), potential->impl.t.as<float2>() + slice * N, N * sizeof(float2),
                              cudaMemcpyDeviceToHost));
         for (long long i = 0; i < N; ++i) {
@@ -348,11 +349,46 @@ int simk_probe_spectrum(simk_context* ctx, const simk_grid* grid, const simk_pro
         DeviceBuffer f32, f64;
         probe_spectrum_device(ctx->impl, g, *probe, f32, &f64);
         std::vector<double2> h(g.count());
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));  // the copy below is not ordered after that stream
         SIMK_CUDA(cudaMemcpy(h.data(), f64.ptr, g.count() * sizeof(double2), cudaMemcpyDeviceToHost));
         for (long long i = 0; i < g.count(); ++i) {
             re[i] = h[i].x;
             im[i] = h[i].y;
         }
+    });
+}
+
+int simk_ctf_kernel(simk_context* ctx, const simk_grid* grid, double energy, const simk_ctf* ctf, double* re,
+                    double* im) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && ctf && re && im, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        GridGeom g = geom_of(grid);
+        DeviceBuffer f64;
+        ctf_kernel_device(ctx->impl, g, energy, *ctf, f64);
+        std::vector<double2> h(g.count());
+        SIMK_CUDA(cudaMemcpyAsync(h.data(), f64.ptr, g.count() * sizeof(double2), cudaMemcpyDeviceToHost,
+                                  ctx->impl.stream));
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+        for (long long i = 0; i < g.count(); ++i) {
+            re[i] = h[i].x;
+            im[i] = h[i].y;
+        }
+    });
+}
+
+int simk_apply_ctf(simk_context* ctx, const simk_grid* grid, double energy, const simk_ctf* ctf, int32_t count,
+                   const double* in_re, const double* in_im, double* out_re, double* out_im, double* out_intensity) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && ctf, "null argument");
+        SIMK_REQUIRE(count >= 0, "negative count");
+        if (count == 0) return;
+        SIMK_REQUIRE(in_re && in_im, "null input");
+        SIMK_REQUIRE((out_re == nullptr) == (out_im == nullptr), "give both out_re and out_im, or neither");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        apply_ctf_device(ctx->impl, geom_of(grid), energy, *ctf, count, in_re, in_im, out_re, out_im, out_intensity);
     });
 }
 
@@ -571,6 +607,7 @@ int simk_finite_profile(simk_context* ctx, int32_t n, const int32_t* atomic_numb
         std::vector<double> r(rho, rho + n), l(zl, zl + n), u(zu, zu + n);
         DeviceBuffer d(n * sizeof(double));
         surrogate_quadrature_points(ctx->impl, z, r, l, u, d.as<double>());
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));  // the copy below is not ordered after that stream
         SIMK_CUDA(cudaMemcpy(out, d.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
     });
 }

@@ -200,6 +200,9 @@ struct KernelTimer {
 void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice, int n_atoms, const int* Z,
                                 const double* xyz, const int* slice_of_atom);
 void prepare_transmissions(Context& ctx, PotentialImpl& pot, double energy);
+void ctf_kernel_device(Context& ctx, const GridGeom& g, double energy, const simk_ctf& ctf, DeviceBuffer& out_f64);
+void apply_ctf_device(Context& ctx, const GridGeom& g, double energy, const simk_ctf& ctf, int count,
+                      const double* in_re, const double* in_im, double* out_re, double* out_im, double* out_intensity);
 void probe_spectrum_device(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
                            DeviceBuffer* out_f64);
 void launch_ramps(Context& ctx, const GridGeom& g, const double* positions_dev, long long first, int count,

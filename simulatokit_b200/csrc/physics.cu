@@ -346,6 +346,132 @@ __global__ void k_probe_spectrum(double2* out, GridDev g, ProbeDev p) {
     }
 }
 
+// ---- contrast transfer function (ContrastTransferFunction.swift:12-115) -------------------------------------------
+// d chi / d alpha and abTEM's azimuthal term, in the coefficient order of chi_of.
+__device__ double dchi_dalpha(double a, double p, const double* c, double lambda) {
+    const double a2 = a * a, a3 = a2 * a, a4 = a3 * a, a5 = a4 * a;
+    const double t1 = (c[1] * cos(2 * (p - c[2])) + c[0]) * a;
+    const double t2 = (c[5] * cos(3 * (p - c[6])) + c[3] * cos(1 * (p - c[4]))) * a2;
+    const double t3 = (c[10] * cos(4 * (p - c[11])) + c[8] * cos(2 * (p - c[9])) + c[7]) * a3;
+    const double t4 = (c[16] * cos(5 * (p - c[17])) + c[14] * cos(3 * (p - c[15])) + c[12] * cos(1 * (p - c[13]))) * a4;
+    const double t5 = (c[23] * cos(6 * (p - c[24])) + c[21] * cos(4 * (p - c[22])) + c[19] * cos(2 * (p - c[20])) +
+                       c[18]) * a5;
+    return 2 * M_PI / lambda * (t1 + t2 + t3 + t4 + t5);
+}
+__device__ double dchi_dphi(double a, double p, const double* c, double lambda) {
+    const double a2 = a * a, a3 = a2 * a, a4 = a3 * a, a5 = a4 * a;
+    const double t1 = 1 / 2.0 * (2.0 * c[1] * sin(2.0 * (p - c[2]))) * a;
+    const double t2 = 1 / 3.0 * (3.0 * c[5] * sin(3.0 * (p - c[6])) + 1.0 * c[3] * sin(1.0 * (p - c[4]))) * a2;
+    const double t3 = 1 / 4.0 * (4.0 * c[10] * sin(4.0 * (p - c[11])) + 2.0 * c[8] * sin(2.0 * (p - c[9]))) * a3;
+    const double t4 = 1 / 5.0 * (5.0 * c[16] * sin(5.0 * (p - c[17])) + 3.0 * c[14] * sin(3.0 * (p - c[15])) +
+                                 1.0 * c[12] * sin(1.0 * (p - c[13]))) * a4;
+    const double t5 = (1 / 6.0) * (6.0 * c[23] * sin(6.0 * (p - c[24])) + 4.0 * c[21] * sin(4.0 * (p - c[22])) +
+                                   2.0 * c[19] * sin(2.0 * (p - c[20]))) * a5;
+    return -2 * M_PI / lambda * (t1 + t2 + t3 + t4 + t5);
+}
+
+struct CtfDev {
+    double lambda, cutoff, dax, day, focal, beta;
+    int soft, infinite;
+    double ab[25];
+};
+
+// H = exp(-i chi) x E_s (beta != 0) x E_t (Delta != 0) x aperture (finite cutoff), float64, FFT order.
+__global__ void k_ctf_kernel(double2* out, GridDev g, CtfDev c) {
+    const long long N = (long long)g.nx * g.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / g.ny), iy = (int)(i % g.ny);
+        const double kx = fftfreq_at(ix, g.nx, g.dx), ky = fftfreq_at(iy, g.ny, g.dy);
+        const double alpha = sqrt(kx * kx + ky * ky) * c.lambda;
+        const double phi = atan2(ky, kx);
+        double s, co;
+        sincos(-chi_of(alpha, phi, c.ab, c.lambda), &s, &co);
+        double f = 1.0;
+        if (c.beta != 0.0) {
+            const double b = c.beta / 1e3;
+            const double dk = dchi_dalpha(alpha, phi, c.ab, c.lambda), dp = dchi_dphi(alpha, phi, c.ab, c.lambda);
+            const double sign = b > 0 ? 1.0 : (b < 0 ? -1.0 : 0.0);
+            f *= exp(-sign * (b / 2) * (b / 2) * (dk * dk + dp * dp));
+        }
+        if (c.focal != 0.0) {
+            const double x = 0.5 * M_PI / c.lambda * c.focal * alpha * alpha;
+            f *= exp(-(x * x));
+        }
+        if (!c.infinite) {
+            double ap;
+            if (c.soft) {
+                if (ix == 0 && iy == 0) ap = 1.0;
+                else {
+                    const double a = cos(phi) * c.dax, b = sin(phi) * c.day;
+                    ap = fmin(fmax((c.cutoff - alpha) / sqrt(a * a + b * b) + 0.5, 0.0), 1.0);
+                }
+            } else ap = (alpha <= c.cutoff) ? 1.0 : 0.0;
+            f *= ap;
+        }
+        out[i] = make_double2(co * f, s * f);
+    }
+}
+
+void ctf_kernel_device(Context& ctx, const GridGeom& g, double energy, const simk_ctf& ctf, DeviceBuffer& out_f64) {
+    SIMK_REQUIRE(std::isfinite(energy) && energy > 0, "the energy must be finite and positive");
+    SIMK_REQUIRE(ctf.semiangle_mrad > 0 && !std::isnan(ctf.semiangle_mrad), "invalid aperture");
+    for (int i = 0; i < 25; ++i) SIMK_REQUIRE(std::isfinite(ctf.aberrations[i]), "every aberration must be finite");
+    SIMK_REQUIRE(std::isfinite(ctf.focal_spread) && ctf.focal_spread >= 0, "focal spread must be finite and >= 0 A");
+    SIMK_REQUIRE(std::isfinite(ctf.angular_spread) && ctf.angular_spread >= 0,
+                 "angular spread must be finite and >= 0 mrad");
+    const long long N = g.count();
+    CtfDev c{};
+    c.lambda = wavelength(energy);
+    c.infinite = std::isinf(ctf.semiangle_mrad) ? 1 : 0;
+    c.soft = ctf.soft ? 1 : 0;
+    c.cutoff = ctf.semiangle_mrad * 1e-3;
+    const double rsx = 1.0 / ((double)g.nx * g.dx()), rsy = 1.0 / ((double)g.ny * g.dy());
+    c.dax = rsx * 1e3 * c.lambda * 1e-3;
+    c.day = rsy * 1e3 * c.lambda * 1e-3;
+    c.focal = ctf.focal_spread;
+    c.beta = ctf.angular_spread;
+    for (int i = 0; i < 25; ++i) c.ab[i] = ctf.aberrations[i];
+    out_f64.alloc(N * sizeof(double2));
+    k_ctf_kernel<<<blocks_for(N), 256, 0, ctx.stream>>>(out_f64.as<double2>(), grid_dev(g), c);
+    ++ctx.launches;
+    SIMK_CUDA(cudaGetLastError());
+}
+
+// Waves.applying: IFFT(FFT(psi) H) on batches of waves in float32 with the float64-computed kernel (1/N folded in).
+void apply_ctf_device(Context& ctx, const GridGeom& g, double energy, const simk_ctf& ctf, int count,
+                      const double* in_re, const double* in_im, double* out_re, double* out_im, double* out_intensity) {
+    const long long N = g.count();
+    DeviceBuffer h64, h32(N * sizeof(float2));
+    ctf_kernel_device(ctx, g, energy, ctf, h64);
+    k_to_float2<<<blocks_for(N), 256, 0, ctx.stream>>>(h32.as<float2>(), h64.as<double2>(), N);
+    ++ctx.launches;
+    SIMK_CUDA(cudaGetLastError());
+    const long long B = std::max<long long>(1, std::min<long long>(count, (256LL << 20) / (N * (long long)sizeof(float2))));
+    DeviceBuffer psi(B * N * sizeof(float2));
+    std::vector<float2> h(B * N);
+    const LinePlan& prow = ctx.plan(g.ny, 32);
+    const LinePlan& pcol = ctx.plan(g.nx, 32);
+    for (long long first = 0; first < count; first += B) {
+        const int b = (int)std::min<long long>(B, count - first);
+        for (long long i = 0; i < b * N; ++i)
+            h[i] = make_float2((float)in_re[first * N + i], (float)in_im[first * N + i]);
+        SIMK_CUDA(cudaMemcpyAsync(psi.ptr, h.data(), b * N * sizeof(float2), cudaMemcpyHostToDevice, ctx.stream));
+        fft2(prow, pcol, psi.ptr, g.nx, g.ny, b, -1, 1.0, ctx.stream, &ctx.launches);
+        launch_mul_broadcast(ctx, psi.as<float2>(), h32.as<float2>(), N, b, 1.0f / (float)N);
+        fft2(prow, pcol, psi.ptr, g.nx, g.ny, b, +1, 1.0, ctx.stream, &ctx.launches);
+        SIMK_CUDA(cudaMemcpyAsync(h.data(), psi.ptr, b * N * sizeof(float2), cudaMemcpyDeviceToHost, ctx.stream));
+        SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+        for (long long i = 0; i < b * N; ++i) {
+            const double re = h[i].x, im = h[i].y;
+            if (out_re) {
+                out_re[first * N + i] = re;
+                out_im[first * N + i] = im;
+            }
+            if (out_intensity) out_intensity[first * N + i] = re * re + im * im;
+        }
+    }
+}
+
 // One block: the float64 sum of |a|^2 in a fixed order (deterministic).
 __global__ void k_norm2(const double2* a, long long N, double* out) {
     __shared__ double part[1024];

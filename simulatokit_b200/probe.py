@@ -1,4 +1,5 @@
-"""Illumination and scan geometry (Sources/SimulatoProbe/): Aperture, Aberrations, Probe, GridScan."""
+"""Illumination, imaging and scan geometry (Sources/SimulatoProbe/): Aperture, Aberrations, Probe, GridScan,
+ContrastTransferFunction."""
 
 from __future__ import annotations
 
@@ -128,3 +129,87 @@ class GridScan:
         xs = self.linspace(self.start[0], self.end[0], self.nx, self.endpoint)
         ys = self.linspace(self.start[1], self.end[1], self.ny, self.endpoint)
         return np.stack(np.meshgrid(xs, ys, indexing="ij"), axis=-1).reshape(-1, 2)
+
+
+class ContrastTransferFunction:
+    """An objective lens (abTEM's CTF; ContrastTransferFunction.swift:37-160): the aberration phase exp(-i chi), the
+    spatial (angular spread beta [mrad]) and temporal (focal spread Delta [A]) envelopes of the quasi-coherent
+    approximation, and the aperture (semiangle [mrad], inf for none). The kernel is computed in float64 on the device;
+    `apply` is Waves.applying (IFFT(FFT(psi) H)) for a batch of waves, float32, returning the waves and the images."""
+
+    def __init__(self, aberrations: Aberrations | None = None, semiangle_cutoff: float = math.inf,
+                 soft_aperture: bool = True, focal_spread: float = 0.0, angular_spread: float = 0.0):
+        if not (semiangle_cutoff > 0) or math.isnan(semiangle_cutoff):
+            _refuse(f"invalid aperture {semiangle_cutoff}")
+        if not (math.isfinite(focal_spread) and focal_spread >= 0):
+            _refuse(f"focal spread must be finite and >= 0 A, got {focal_spread}")
+        if not (math.isfinite(angular_spread) and angular_spread >= 0):
+            _refuse(f"angular spread must be finite and >= 0 mrad, got {angular_spread}")
+        self.aberrations = aberrations or Aberrations()
+        self.semiangle_cutoff = float(semiangle_cutoff)
+        self.soft_aperture = bool(soft_aperture)
+        self.focal_spread = float(focal_spread)
+        self.angular_spread = float(angular_spread)
+
+    def c(self):
+        return L.Ctf_t((C.c_double * 25)(*self.aberrations.array()), self.semiangle_cutoff,
+                       1 if self.soft_aperture else 0, 0, self.focal_spread, self.angular_spread)
+
+    def kernel(self, grid: Grid, energy: float, engine: Engine | None = None) -> np.ndarray:
+        """H on the grid in FFT order (ContrastTransferFunction.kernel, :85-115)."""
+        e = engine or Engine.require()
+        re = np.zeros(grid.nx * grid.ny)
+        im = np.zeros(grid.nx * grid.ny)
+        g, c = grid.c(), self.c()
+        L.check(e.lib.simk_ctf_kernel(e.handle, C.byref(g), float(energy), C.byref(c), L.dptr(re), L.dptr(im)))
+        return (re + 1j * im).reshape(grid.nx, grid.ny)
+
+    def apply(self, waves, engine: Engine | None = None):
+        """Waves.applying (:146-161) on one Waves or a list of waves of one grid and beam: (waves, images)."""
+        e = engine or Engine.require()
+        many = isinstance(waves, (list, tuple))
+        ws = list(waves) if many else [waves]
+        if not ws:
+            return ([], []) if many else (None, None)
+        grid, beam = ws[0].grid, ws[0].beam
+        for w in ws:
+            if not w.grid.matches(grid) or w.beam.energy != beam.energy:
+                _refuse("the waves must share one grid and beam")
+        n = grid.nx * grid.ny
+        stack = np.ascontiguousarray(np.stack([w.field for w in ws]).reshape(len(ws), n))
+        re_in, im_in = np.ascontiguousarray(stack.real), np.ascontiguousarray(stack.imag)
+        re, im, inten = np.zeros(len(ws) * n), np.zeros(len(ws) * n), np.zeros(len(ws) * n)
+        g, c = grid.c(), self.c()
+        L.check(e.lib.simk_apply_ctf(e.handle, C.byref(g), float(beam.energy), C.byref(c), len(ws), L.dptr(re_in),
+                                     L.dptr(im_in), L.dptr(re), L.dptr(im), L.dptr(inten)))
+        out = [Waves((re[k * n:(k + 1) * n] + 1j * im[k * n:(k + 1) * n]).reshape(grid.nx, grid.ny), grid, w.beam,
+                     w.normalization) for k, w in enumerate(ws)]
+        images = [inten[k * n:(k + 1) * n].reshape(grid.nx, grid.ny) for k in range(len(ws))]
+        return (out, images) if many else (out[0], images[0])
+
+    @staticmethod
+    def scherzer_defocus(Cs: float, energy: float, factor: float = 1.5) -> float:
+        """sign(Cs) sqrt(factor |Cs| lambda) [A] (:118-124)."""
+        if not (math.isfinite(factor) and factor > 0):
+            _refuse("the Scherzer factor must be finite and positive")
+        lam = ElectronBeam(energy).wavelength
+        s = 1.0 if Cs > 0 else (-1.0 if Cs < 0 else 0.0)
+        return s * math.sqrt(factor * abs(Cs) * lam)
+
+    @staticmethod
+    def point_resolution(Cs: float, energy: float, divisor: float = 6.0) -> float:
+        """(lambda^3 |Cs| / divisor)^(1/4) [A] (:127-131)."""
+        if not (math.isfinite(divisor) and divisor > 0):
+            _refuse("the divisor must be finite and positive")
+        lam = ElectronBeam(energy).wavelength
+        return math.pow(math.pow(lam, 3) * abs(Cs) / divisor, 1.0 / 4)
+
+    @staticmethod
+    def nyquist_sampling(semiangle_cutoff: float, energy: float, oversampling: float = 4.0) -> float:
+        """1 / (oversampling alpha_c / lambda 1e-3) [A] (:134-142)."""
+        if not (math.isfinite(semiangle_cutoff) and semiangle_cutoff > 0):
+            _refuse(f"invalid aperture {semiangle_cutoff}")
+        if not (math.isfinite(oversampling) and oversampling > 0):
+            _refuse(f"invalid oversampling {oversampling}")
+        lam = ElectronBeam(energy).wavelength
+        return 1 / (oversampling * semiangle_cutoff / lam * 1e-3)

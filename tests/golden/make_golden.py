@@ -28,6 +28,7 @@ KEEP = {
                 "B2/probe.incident"],
     "slice-2": None,   # all (1.4 MB)
     "slice-4": None,
+    "slice-3": None,   # CTF kernels and HRTEM images (1.5 MB)
     "slice-4-scan": ["com_mrad", "com_inv", "dp"],
     "waves": None,     # all six runs (1.5 MB): full size and five Fourier resamplings
 }

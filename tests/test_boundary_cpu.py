@@ -144,3 +144,22 @@ def test_waves_detector_refusals_on_the_host():
         sk.STEM.scan(probe, pots, scan, sk.WavesDetector())
     with pytest.raises(sk.InvalidArgument, match="one potential, got 0"):
         sk.STEM.scan(probe, [], scan, sk.WavesDetector())
+
+
+def test_ctf_closed_forms_on_the_host():
+    """Scherzer defocus, point resolution and Nyquist sampling (ContrastTransferFunction.swift:118-142) against the
+    reference's pins at 1e-15, and its textbook values (CTFTests.closedFormsEqualAbTEMAndTheTextbook)."""
+    import simulatokit_b200 as sk
+    CTF = sk.ContrastTransferFunction
+    s3 = G.pins()["slice-3"]
+    for row in s3["closed_forms"]:
+        assert abs(CTF.scherzer_defocus(row["Cs"], row["energy"]) - row["scherzer"]) <= 1e-15 * abs(row["scherzer"])
+        assert abs(CTF.point_resolution(row["Cs"], row["energy"]) - row["point_resolution"]) <= \
+            1e-15 * row["point_resolution"]
+    for row in s3["nyquist"]:
+        assert abs(CTF.nyquist_sampling(row["semiangle"], row["energy"]) - row["sampling"]) <= 1e-15 * row["sampling"]
+    assert abs(CTF.scherzer_defocus(1.2e7, 200e3) - 671.9) < 0.05
+    assert abs(CTF.point_resolution(1.2e7, 200e3) - 2.370) < 0.0005
+    assert abs(CTF.nyquist_sampling(20, 200e3) - 0.3135) < 0.00005
+    with pytest.raises(sk.InvalidArgument):
+        CTF(focal_spread=-1.0)

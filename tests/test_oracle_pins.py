@@ -288,3 +288,46 @@ def test_resample_map_round_trip():
     up = O.resample_wave(psi, 25, 16)
     back = O.resample_wave(up, 12, 9)
     assert np.max(np.abs(back - psi)) <= 1e-12 * np.max(np.abs(psi))
+
+
+def _ctf_case(cid):
+    c = G.pins()["slice-3"]["cases"][cid]
+    g = O.Grid(c["gpts"][0], c["gpts"][1], c["extent"][0], c["extent"][1])
+    cutoff = c["cutoff_mrad"] if c["cutoff_mrad"] is not None else math.inf
+    return c, g, dict(ab=c["aberrations"], cutoff_mrad=cutoff, soft=c["soft"], focal_spread=c["focal_spread"],
+                      angular_spread=c["angular_spread"])
+
+
+@pytest.mark.parametrize("cid", ["H1", "H2", "H3", "K1", "K2"])
+def test_ctf_kernels(cid):
+    """CTFTests.kernelsEqualAbTEM (Probe/CTFTests.swift): the kernel (phase, envelopes, aperture) at 1e-12 max-relative."""
+    c, g, kw = _ctf_case(cid)
+    h = O.ctf_kernel(g, c["energy"], **kw)
+    assert O.rel_max(h, G.array("slice-3", f"{cid}.kernel")) <= 1e-12
+
+
+def _srtio3_exit(pi_choice):
+    s = O.srtio3_cell().repeated(3, 3, 5)
+    op = O.Potential.from_structure(s, 120, 120, slice_thickness=1.9525, pi_choice=pi_choice)
+    ts = [O.transmission(v, 300e3, op.grid) for v in op.build()]
+    return O.multislice(O.plane_wave(op.grid), ts, op.thicknesses, 300e3, op.grid)[-1], op.grid
+
+
+@pytest.mark.parametrize("pi_choice,bound", [("abtem", 1e-10), ("exact", 1e-6)])
+def test_hrtem_images(pi_choice, bound):
+    """CTFTests.hrtemImagesEqualAbTEM: |IFFT(FFT(exit) H)|^2 of the SrTiO3 3x3x5 exit wave for H1-H3."""
+    ex, g = _srtio3_exit(pi_choice)
+    for cid in ("H1", "H2", "H3"):
+        c, _, kw = _ctf_case(cid)
+        img = np.abs(O.apply_ctf(ex, O.ctf_kernel(g, c["energy"], **kw))) ** 2
+        assert O.rel_max(img, G.array("slice-3", f"{cid}.image")) <= bound, cid
+
+
+def test_ctf_closed_forms():
+    s3 = G.pins()["slice-3"]
+    for row in s3["closed_forms"]:
+        assert abs(O.scherzer_defocus(row["Cs"], row["energy"]) - row["scherzer"]) <= 1e-15 * abs(row["scherzer"])
+        assert abs(O.point_resolution(row["Cs"], row["energy"]) - row["point_resolution"]) <= \
+            1e-15 * row["point_resolution"]
+    for row in s3["nyquist"]:
+        assert abs(O.nyquist_sampling(row["semiangle"], row["energy"]) - row["sampling"]) <= 1e-15 * row["sampling"]
