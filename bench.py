@@ -16,8 +16,10 @@ the device -> scan -> detector images back to the host), wall-clocked per call.
 stages) on the same stream, and, with the CPU leg, each form's relative L2 error per detector image against the float64
 oracle at the CPU leg's sample positions (the bound for every form is 1e-4).
 
-`--impl reference`: the reference's CPU path (restated in float64 NumPy, oracle/simk_oracle.py; the Swift original
-cannot build on Linux) timed on the host cores on a bounded sample of positions of the same workload.
+`--impl reference` and the `cpu_baseline` leg: the reference's CPU path restated in C++17 float64
+(oracle/cpu/simk_cpu.cpp: its mixed-radix / Bluestein FFT2D, runCPU, Probe.build and the annular detectors, checked
+against the float64 NumPy oracle; the Swift original cannot build on Linux), timed on min(8, cores) host threads over
+positions on a bounded sample of positions of the same workload.
 """
 
 from __future__ import annotations
@@ -204,10 +206,12 @@ def sample_indices(n_positions: int):
 
 
 def cpu_reference(n_positions: int, threads: int, want_values: bool = False):
-    """Times the float64 CPU restatement of STEM.cpuScan on `n_positions` positions of the workload (transmissions
-    computed once, as runBatch shares them), `threads` positions at a time. Returns (steps/s, seconds, positions) and,
-    with want_values, the detector values at those positions ([detector][position])."""
-    from concurrent.futures import ThreadPoolExecutor
+    """Times the C++ float64 restatement of STEM.cpuScan (oracle/cpu/simk_cpu.cpp: FFT2D's mixed-radix / Bluestein
+    transforms, runCPU, Probe.build, the annular detectors) on `n_positions` positions of the workload, `threads`
+    workers over positions as runCPUParallel. The transmissions, propagators, probe spectrum and masks are built once
+    beforehand (float64 NumPy oracle), as runBatch shares them. Returns (steps/s, seconds, positions) and, with
+    want_values, the detector values at those positions ([detector][position])."""
+    from oracle import simk_cpu as K
     from oracle import simk_oracle as O
     box, nums, pos = srtio3(8, 8, 20)
     s = O.Structure(box, nums, pos)
@@ -215,24 +219,20 @@ def cpu_reference(n_positions: int, threads: int, want_values: bool = False):
     g = p.grid
     ts = [O.transmission(v, ENERGY, g) for v in p.build()]
     spec = O.ProbeSpec(ENERGY, SEMIANGLE)
-    dets = [O.DetectorSpec("annular", {"inner": a, "outer": b}) for _, a, b in DETECTORS]
+    inputs = K.ScanInputs(spec, g, ts, p.thicknesses, K.annular_masks(g, ENERGY, [(a, b) for _, a, b in DETECTORS]))
     positions = scan_positions()[sample_indices(n_positions)]
-
-    def one(q):
-        psi0 = O.build_probe(spec, g, positions[q])
-        ex = O.multislice(psi0, ts, p.thicknesses, ENERGY, g)[-1]
-        pat = O.diffraction_intensity(ex)
-        return [d.detect(pat, g, ENERGY) for d in dets]
-
-    one(0)  # warm-up
+    inputs.scan(positions[:1], threads=1)  # warm-up
     t0 = time.perf_counter()
-    with ThreadPoolExecutor(threads) as ex:
-        vals = list(ex.map(one, range(len(positions))))
+    vals = inputs.scan(positions, threads=threads)
     dt = time.perf_counter() - t0
     out = (len(positions) * len(p.thicknesses) / dt, dt, len(positions))
     if want_values:
-        return out + ([np.array([v[d][0] for v in vals]) for d in range(len(dets))],)
+        return out + ([vals[:, d].copy() for d in range(len(DETECTORS))],)
     return out
+
+
+CPU_SAMPLE = ("{n} of 4096 positions x 20 slices per step, C++17 float64 restatement of STEM.cpuScan "
+              "(oracle/cpu/simk_cpu.cpp), {threads} threads over positions")
 
 
 def run_reference(args):
@@ -253,8 +253,7 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference", "config": {"workload": WORKLOAD, "form": "cpu float64"},
             "cpu_baseline": {"value": value, "unit": "probe.slice steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{n} of 4096 positions x 20 slices per step, float64 NumPy restatement of "
-                                       f"STEM.cpuScan, {threads} threads over positions"},
+                             "sample": CPU_SAMPLE.format(n=n, threads=threads)},
             "e2e": {"value": value, "unit": "probe.slice steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -714,15 +713,14 @@ def main():
         threads = min(8, os.cpu_count() or 1)
         v, dt, n, ref_vals = cpu_reference(args.cpu_positions, threads, want_values=True)
         cpu = {"value": v, "unit": "probe.slice steps/s", "cores": threads, "kind": "port",
-               "sample": f"{n} of 4096 positions x 20 slices ({dt:.1f} s), float64 NumPy restatement of STEM.cpuScan, "
-                         f"{threads} threads over positions"}
+               "sample": CPU_SAMPLE.format(n=n, threads=threads) + f" ({dt:.1f} s)"}
         idx = sample_indices(args.cpu_positions)
         for f, vals in form_values.items():
             errs = [float(np.linalg.norm(vals[d][idx] - ref_vals[d]) / np.linalg.norm(ref_vals[d]))
                     for d in range(len(dets))]
             forms[f]["rel_l2_vs_fp64"] = dict(zip([name for name, _, _ in DETECTORS], errs))
         if forms:
-            forms["error_sample"] = f"detector values at the {n} CPU sample positions vs the float64 oracle"
+            forms["error_sample"] = f"detector values at the {n} CPU sample positions vs the C++ float64 restatement"
 
     if rank == 0:
         line = {"metric": "probe.slice steps/s", "value": value, "unit": "probe.slice steps/s", "n_gpus": world,
