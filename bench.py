@@ -281,7 +281,8 @@ def _device_scan(sk, L, engine, probe, pots, positions, dets, torch):
     return run, outs
 
 
-def _time_scans(engine, run, steps, warmup, stream, torch, local):
+def _time_scans(engine, run, steps, warmup, stream, torch, local,
+                names=("fused_rows", "fused_cols", "line_fft", "pointwise", "detect")):
     for _ in range(warmup):
         run()
     torch.cuda.synchronize()
@@ -301,13 +302,12 @@ def _time_scans(engine, run, steps, warmup, stream, torch, local):
     engine.kernel_time("fused_cols", reset=True)
     run()
     torch.cuda.synchronize()
-    names = ["fused_rows", "fused_cols", "line_fft", "pointwise", "detect"]
     kt = {n: engine.kernel_time(n) for n in names}
     engine.set_timing(False)
     return ms, launches, clocks.summary(), kt
 
 
-def _roofline(kt, n):
+def _roofline(kt, n, step_rule=None):
     dom = max(kt, key=lambda k: kt[k][0])
     dms, dn, dbytes = kt[dom]
     peak, kind = measured_peaks()
@@ -319,7 +319,7 @@ def _roofline(kt, n):
             "traffic": None, "algorithmic_bytes_per_launch": dbytes / dn if dn else None,
             "avg_launch_ms": dms / dn if dn else None,
             "kernel_share": {k: round(v[0] / total, 4) for k, v in kt.items() if v[1]},
-            "step_bytes_rule": f"32*N bytes per probe.slice step, N = {n}x{n}"}
+            "step_bytes_rule": step_rule or f"32*N bytes per probe.slice step, N = {n}x{n}"}
 
 
 def run_4dstem(args, sk, L, engine, stream, torch, local):
@@ -509,6 +509,88 @@ def run_jobs(args, sk, L, engine, stream, torch, local):
             "roofline": None, "cpu_baseline": None, "clocks": None, "gpu_launches": None}
 
 
+def run_scanops(args, sk, L, engine, stream, torch, local):
+    """Scan post-processing of a 4D-STEM measurement kept on the device: N x N positions (--post-scan, default 64) x
+    128 x 128 binned values (float64; 537 MB at 64; synthetic patterns, each summing to 1), the Gaussian source size
+    (sigma 0.5 A on 0.2 A scan pixels: 2.5 pixels, 21 taps per axis) then Poisson noise at 1e5 electrons per pattern
+    (mean 6.1 per value: Knuth's sampler), in place; one step = a device copy of the measurement and both operations.
+    The integrated centre of mass of a 256 x 256 COM scan is timed beside it. value = post-processed values per
+    second."""
+    import ctypes as C
+    ns, nv = args.post_scan, 128
+    count = ns * ns * nv * nv
+    sigma, samp, dose = 0.5, 0.2, 1e5
+    g = torch.Generator(device="cuda").manual_seed(1)
+    base = torch.rand((ns * ns, nv * nv), dtype=torch.float64, device="cuda", generator=g)
+    base /= base.sum(dim=1, keepdim=True)
+    work = torch.empty_like(base)
+
+    def run():
+        work.copy_(base)
+        p = C.c_void_p(work.data_ptr())
+        L.check(engine.lib.simk_gaussian_source_size_device(engine.handle, ns, ns, nv * nv, sigma, sigma, samp, samp,
+                                                            p, p))
+        L.check(engine.lib.simk_poisson_noise_device(engine.handle, count, p, dose, 1, 7, p))
+
+    ms, launches, clocks, kt = _time_scans(engine, run, args.steps, args.warmup, stream, torch, local,
+                                           names=("gauss_axis", "poisson"))
+    value = count * args.steps / (ms / 1e3)
+    roof = _roofline({"gauss_axis": kt["gauss_axis"]}, 0, step_rule="16 B per value per axis pass (read + write)")
+    total_ms = sum(v[0] for v in kt.values())
+    roof["kernel_share"] = {k: round(v[0] / total_ms, 4) for k, v in kt.items() if v[1]}
+    pois_ms, pois_n, _ = kt["poisson"]
+    # iCOM of a 256 x 256 centre-of-mass scan (interleaved pairs, stride 2)
+    com = torch.rand(256 * 256 * 2, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    icom = torch.empty(256 * 256, dtype=torch.float64, device="cuda")
+
+    def run_icom():
+        L.check(engine.lib.simk_integrate_gradient_device(engine.handle, 256, 256, 0.1, 0.1,
+                                                          C.c_void_p(com.data_ptr()), C.c_void_p(com.data_ptr() + 8),
+                                                          2, C.c_void_p(icom.data_ptr())))
+    for _ in range(3):
+        run_icom()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(20):
+        run_icom()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    icom_ms = e0.elapsed_time(e1) / 20
+    # end to end: host arrays through the package's ScanMeasurement methods (copies in and out each call)
+    host = base.reshape(-1).cpu().numpy()
+    m = sk.ScanMeasurement([ns, ns], [nv, nv], host)
+    m.gaussianSourceSize(sigma, samplingX=samp, samplingY=samp, engine=engine)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        m.gaussianSourceSize(sigma, samplingX=samp, samplingY=samp, engine=engine).poissonNoise(dose, seed=7,
+                                                                                              engine=engine)
+    e2e_s = (time.perf_counter() - t0) / 2
+    cpu = None
+    if not args.no_cpu:
+        # the oracle's float64 Gaussian filter on a bounded sample: every position, 256 values each
+        from oracle import simk_oracle as O
+        sample = host.reshape(ns, ns, nv * nv)[:, :, :256].copy()
+        t0 = time.perf_counter()
+        O.gaussian_source_size(sample, [ns, ns], sigma, sigma, samp, samp)
+        dt = time.perf_counter() - t0
+        cpu = {"value": sample.size / dt, "unit": "values/s", "cores": 1, "kind": "port",
+               "sample": f"Gaussian source size only, {ns}x{ns} positions x 256 values ({dt:.2f} s), float64 NumPy "
+                         "restatement of ScanMeasurement.gaussianSourceSize"}
+    return {"metric": "post-processed values/s", "unit": "values/s", "value": value, "ms_per_step": ms / args.steps,
+            "dtype": "f64",
+            "config": {"workload": f"scan post-processing of a 4D-STEM measurement on the device: {ns}x{ns} positions "
+                                   f"x 128x128 values (float64, {8 * count / 1e6:.0f} MB), Gaussian source size sigma "
+                                   "0.5 A at 0.2 A scan pixels (21 taps per axis) + Poisson noise at 1e5 e per "
+                                   "pattern, in place", "values": count,
+                       "inputs": "larger than L2 at the default size (537 MB), no flush"},
+            "roofline": roof, "poisson": {"avg_launch_ms": pois_ms / pois_n if pois_n else None,
+                                          "values_per_s": count / (pois_ms / pois_n / 1e3) if pois_n else None},
+            "icom_256x256_ms": icom_ms, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "e2e": {"value": count / e2e_s, "unit": "values/s", "h2d_bytes_per_step": 8 * count * 2,
+                    "d2h_bytes_per_step": 8 * count * 2}}
+
+
 def run_extra(args):
     import torch
     import simulatokit_b200 as sk
@@ -523,11 +605,12 @@ def run_extra(args):
     engine.set_stream(stream.cuda_stream)
     engine.apply(sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma,
                              autotune=args.autotune))
-    fn = {"4dstem": run_4dstem, "surrogate": run_surrogate, "jobs": run_jobs}[args.workload]
+    fn = {"4dstem": run_4dstem, "surrogate": run_surrogate, "jobs": run_jobs, "scanops": run_scanops}[args.workload]
     line = fn(args, sk, L, engine, stream, torch, local)
-    line.update({"unit": "probe.slice steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                 "data": "synthetic", "e2e": None})
+    for k, v in {"unit": "probe.slice steps/s", "dtype": "f32", "e2e": None}.items():
+        line.setdefault(k, v)
+    line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                 "scaling": "weak", "vs_baseline": None, "data": "synthetic"})
     print(json.dumps(line), flush=True)
 
 
@@ -550,13 +633,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
-    ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate", "jobs"],
-                    help="stem: the headline STEM HAADF+BF scan; 4dstem, surrogate, jobs: the other configurations")
+    ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate", "jobs", "scanops"],
+                    help="stem: the headline STEM HAADF+BF scan; 4dstem, surrogate, jobs: the other configurations; "
+                         "scanops: scan post-processing of a 4D-STEM measurement")
     ap.add_argument("--sg-samples", type=int, default=10_000_000, help="surrogate workload: quadrature samples")
     ap.add_argument("--sg-steps", type=int, default=20000, help="surrogate workload: training steps")
     ap.add_argument("--jobs-chunk", type=int, default=256, help="jobs workload: jobs per table call")
     ap.add_argument("--configs", type=int, default=16, help="4dstem workload: frozen-phonon configurations")
     ap.add_argument("--scan", type=int, default=48, help="4dstem workload: scan positions per side")
+    ap.add_argument("--post-scan", type=int, default=64, help="scanops workload: scan positions per side")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -252,6 +252,45 @@ int simk_ctf_kernel(simk_context* ctx, const simk_grid* grid, double energy, con
 int simk_apply_ctf(simk_context* ctx, const simk_grid* grid, double energy, const simk_ctf* ctf, int32_t count,
                    const double* in_re, const double* in_im, double* out_re, double* out_im, double* out_intensity);
 
+/* ---- scan post-processing (Sources/SimulatoDetector/ScanOperations.swift, IntegratedCenterOfMass.swift,
+ * Sources/SimulatoCore/ImageOperations.swift) ------------------------------------------------------------------------
+ * On a finished scan's float64 values, row-major [scan x][scan y][value_count] (a ScanMeasurement's layout). Each call
+ * has a host form (host arrays, copied in and out) and a _device form (device pointers, e.g. simk_scan_device's
+ * outputs, which stay on the device); both return when the result is written. */
+
+/* ScanMeasurement.gaussianSourceSize(sigmaX:sigmaY:samplingX:samplingY:) (ScanOperations.swift:19-36): every value
+ * filtered over the nx x ny scan with scipy's periodic Gaussian (radius floor(4 s + 1/2) pixels, s = sigma / sampling,
+ * weights normalised), along y then x; sigma 0 leaves an axis alone. sigma [A] finite and >= 0, sampling [A] finite
+ * and > 0, else SIMK_ERR_INVALID. Bit-equal to the reference's float64 loop. `out` may equal `in`. */
+int simk_gaussian_source_size(simk_context* ctx, int32_t nx, int32_t ny, int64_t value_count, double sigma_x,
+                              double sigma_y, double sampling_x, double sampling_y, const double* in, double* out);
+int simk_gaussian_source_size_device(simk_context* ctx, int32_t nx, int32_t ny, int64_t value_count, double sigma_x,
+                                     double sigma_y, double sampling_x, double sampling_y, const double* in_device,
+                                     double* out_device);
+
+/* ScanMeasurement.poissonNoise(dose:samples:seed:) (ScanOperations.swift:80-117): `samples` draws of the `count` values,
+ * out[s count + i] ~ Poisson(max(in[i] dose, 0)), by the reference's sampler (Knuth below a mean of 10, PTRS above).
+ * poissonNoise(dosePerArea:samplingX:samplingY:...) is dose = samplingX samplingY dosePerArea. The generator differs
+ * from the reference's single stream: every value and sample has its own xoshiro256** seeded by
+ * mix(mix(seed) + s count + i), so a seed gives the same noise on every run, not the reference's draws. dose finite
+ * and >= 0, samples >= 1, finite values, else SIMK_ERR_INVALID. `out` (samples x count) may equal `in` when samples is
+ * 1. */
+int simk_poisson_noise(simk_context* ctx, int64_t count, const double* in, double dose, int32_t samples, uint64_t seed,
+                       double* out);
+int simk_poisson_noise_device(simk_context* ctx, int64_t count, const double* in_device, double dose, int32_t samples,
+                              uint64_t seed, double* out_device);
+
+/* RealField.integratingGradient (ImageOperations.swift:39-48, 140-167) and ScanMeasurement.integratedCenterOfMass
+ * (IntegratedCenterOfMass.swift:36-40): the nx x ny gradient field gx[i stride], gy[i stride] (pixel i = ix ny + iy)
+ * integrated in Fourier space, T^ = (kx g^x + ky g^y) / (2 pi i |k|^2) (|k|^2 = 1e-12 at zero frequency), the real
+ * part of the inverse transform less its minimum, into out[nx ny]. A centre-of-mass measurement's interleaved (x, y)
+ * pairs are gx = values, gy = values + 1, stride 2. nx, ny >= 2 and sampling finite and > 0, else SIMK_ERR_INVALID. */
+int simk_integrate_gradient(simk_context* ctx, int32_t nx, int32_t ny, double sampling_x, double sampling_y,
+                            const double* gx, const double* gy, int64_t stride, double* out);
+int simk_integrate_gradient_device(simk_context* ctx, int32_t nx, int32_t ny, double sampling_x, double sampling_y,
+                                   const double* gx_device, const double* gy_device, int64_t stride,
+                                   double* out_device);
+
 /* ---- job tables ----------------------------------------------------------------------------------------------------
  * No reference counterpart as one call (the reference runs such jobs one Multislice.run at a time, Multislice.swift:52-80
  * -> MetalEngine.swift:458-474); proposed as simk_job_table_run for uneven batches. Each job: an incident plane wave

@@ -1104,3 +1104,155 @@ def surrogate_pack(d: dict) -> np.ndarray:
     return np.concatenate([np.asarray(d[k], dtype=np.float64).ravel()
                            for k in ("emb", "W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4")])
 
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# Scan post-processing (Sources/SimulatoDetector/ScanOperations.swift:12-167, IntegratedCenterOfMass.swift:11-41,
+# Sources/SimulatoCore/ImageOperations.swift:39-48, 140-176)
+# ---------------------------------------------------------------------------------------------------------------------
+
+def gaussian_kernel(sigma_px: float) -> np.ndarray:
+    """scipy's gaussian_filter1d weights (ScanOperations.swift:43-50): exp(-x^2 / 2 s^2) for |x| <= floor(4 s + 1/2),
+    divided by their sum taken in order."""
+    radius = int(4.0 * sigma_px + 0.5)
+    w = [math.exp(-0.5 * float(x * x) / (sigma_px * sigma_px)) for x in range(-radius, radius + 1)]
+    total = 0.0
+    for v in w:
+        total += v
+    return np.array([v / total for v in w])
+
+
+def _filter_axis(data: np.ndarray, axis: int, sigma_px: float) -> np.ndarray:
+    """One periodic pass (ScanOperations.swift:52-72): out[k] = sum_j w[j] in[(k + j - r) mod L], summed in j order."""
+    if not sigma_px > 0:
+        return data
+    w = gaussian_kernel(sigma_px)
+    r = len(w) // 2
+    L = data.shape[axis]
+    src = np.moveaxis(data, axis, 0)
+    out = np.zeros_like(src)
+    for k in range(L):
+        acc = np.zeros(src.shape[1:])
+        for j, wj in enumerate(w):
+            acc = acc + wj * src[(k + j - r) % L]
+        out[k] = acc
+    return np.moveaxis(out, 0, axis)
+
+
+def gaussian_source_size(values: np.ndarray, scan_shape, sigma_x: float, sigma_y: float, sampling_x: float,
+                         sampling_y: float) -> np.ndarray:
+    """ScanMeasurement.gaussianSourceSize (ScanOperations.swift:19-36): the values [nx][ny][...] filtered along the
+    second scan axis with sigma_y / sampling_y pixels, then the first with sigma_x / sampling_x, both periodic."""
+    for v in (sigma_x, sigma_y):
+        if not (math.isfinite(v) and v >= 0):
+            raise ValueError("the source size must be finite and non-negative")
+    for v in (sampling_x, sampling_y):
+        if not (math.isfinite(v) and v > 0):
+            raise ValueError("the scan sampling must be finite and positive")
+    if len(scan_shape) != 2:
+        raise ValueError("the source size filters a two-axis scan")
+    nx, ny = scan_shape
+    d = np.asarray(values, dtype=np.float64).reshape(nx, ny, -1)
+    d = _filter_axis(d, 1, sigma_y / sampling_y)
+    d = _filter_axis(d, 0, sigma_x / sampling_x)
+    return d.reshape(np.shape(values))
+
+
+def integrate_gradient(gx: np.ndarray, gy: np.ndarray, sampling_x: float, sampling_y: float) -> np.ndarray:
+    """integrateGradient (ImageOperations.swift:140-167), abTEM's _integrate_gradient_2d: T^ = (kx g^x + ky g^y) /
+    (2 pi i |k|^2), |k|^2 = 1e-12 at zero frequency, the real part of the inverse transform less its minimum."""
+    for v in (sampling_x, sampling_y):
+        if not (math.isfinite(v) and v > 0):
+            raise ValueError("invalid sampling")
+    gx, gy = np.asarray(gx, dtype=np.float64), np.asarray(gy, dtype=np.float64)
+    nx, ny = gx.shape
+    fx, fy = np.fft.fft2(gx.astype(np.complex128)), np.fft.fft2(gy.astype(np.complex128))
+    kx, ky = fftfreq(nx, sampling_x)[:, None], fftfreq(ny, sampling_y)[None, :]
+    k = kx * kx + ky * ky
+    k = np.where(k == 0, 1e-12, k)
+    a = fx.real * kx + fy.real * ky
+    b = fx.imag * kx + fy.imag * ky
+    c = 2 * math.pi * k
+    t = np.fft.ifft2(b / c - 1j * (a / c)).real
+    return t - t.min()
+
+
+def integrated_center_of_mass(values: np.ndarray, scan_shape, sampling_x: float, sampling_y: float) -> np.ndarray:
+    """ScanMeasurement.integratedCenterOfMass (IntegratedCenterOfMass.swift:36-40): the (x, y) pairs of a
+    centre-of-mass measurement as two images over the scan, integrated."""
+    if len(scan_shape) != 2:
+        raise ValueError("a centre-of-mass image needs a two-axis scan")
+    v = np.asarray(values, dtype=np.float64).reshape(scan_shape[0], scan_shape[1], 2)
+    return integrate_gradient(v[..., 0], v[..., 1], sampling_x, sampling_y)
+
+
+def _uniform(rng: GaussianGenerator) -> float:
+    """PoissonSampler.uniform (ScanOperations.swift:133-135): the top 53 bits over 2^53."""
+    return (rng.next_u64() >> 11) * (1.0 / 9007199254740992.0)
+
+
+def poisson_draw(lam: float, rng: GaussianGenerator) -> int:
+    """PoissonSampler.draw (ScanOperations.swift:137-166): Knuth's product below a mean of 10, Hoermann's PTRS
+    (transformed rejection with squeeze) above."""
+    if lam <= 0:
+        return 0
+    if lam < 10:
+        limit = math.exp(-lam)
+        product, k = _uniform(rng), 0
+        while product > limit:
+            product *= _uniform(rng)
+            k += 1
+        return k
+    slam, loglam = math.sqrt(lam), math.log(lam)
+    b = 0.931 + 2.53 * slam
+    a = -0.059 + 0.02483 * b
+    invalpha = 1.1239 + 1.1328 / (b - 3.4)
+    vr = 0.9277 - 3.6224 / (b - 2)
+    while True:
+        u = _uniform(rng) - 0.5
+        v = _uniform(rng)
+        us = 0.5 - abs(u)
+        if us <= 0:
+            continue
+        kd = math.floor((2 * a / us + b) * u + lam + 0.43)
+        if not (math.isfinite(kd) and abs(kd) < 9e18):
+            continue
+        k = int(kd)
+        if us >= 0.07 and v <= vr:
+            return k
+        if k < 0 or (us < 0.013 and v > us):
+            continue
+        if math.log(v) + math.log(invalpha) - math.log(a / (us * us) + b) <= -lam + k * loglam - math.lgamma(k + 1.0):
+            return k
+
+
+def poisson_noise_sequential(values, dose: float, seed: int, samples: int = 1) -> np.ndarray:
+    """ScanMeasurement.poissonNoise (ScanOperations.swift:80-117): max(value dose, 0) drawn in order from ONE generator
+    stream over every value and sample -- the reference's own bits. Shape (samples, values). Finite values only."""
+    if not (math.isfinite(dose) and dose >= 0):
+        raise ValueError("the dose must be finite and non-negative")
+    rng = GaussianGenerator(seed)
+    means = [max(float(v) * dose, 0.0) for v in np.asarray(values, dtype=np.float64).ravel()]
+    return np.array([[float(poisson_draw(m, rng)) for m in means] for _ in range(samples)])
+
+
+def poisson_value_seed(seed: int, index: int) -> int:
+    """The seed of value `index` (sample s of value i: index s * count + i) in the device's per-value streams: the
+    same mix as a frozen-phonon configuration's seed, mix(mix(seed) + index)."""
+    return configuration_seed(seed, index)
+
+
+def poisson_noise_streams(values, dose: float, seed: int, samples: int = 1) -> np.ndarray:
+    """The device's Poisson noise: max(value dose, 0) drawn by PoissonSampler.draw from a generator of its own per value
+    and sample, seeded by poisson_value_seed. The same seed gives the same noise on every run and any split of the
+    work; the draws are not the reference's sequential stream. Shape (samples, values). Finite values only."""
+    if not (math.isfinite(dose) and dose >= 0):
+        raise ValueError("the dose must be finite and non-negative")
+    v = np.asarray(values, dtype=np.float64).ravel()
+    n = v.size
+    out = np.zeros((samples, n))
+    for s in range(samples):
+        for i in range(n):
+            m = max(float(v[i]) * dose, 0.0)
+            out[s, i] = float(poisson_draw(m, GaussianGenerator(poisson_value_seed(seed, s * n + i)))) if m > 0 else 0.0
+    return out

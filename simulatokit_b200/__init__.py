@@ -8,7 +8,7 @@ every compute call raises CudaUnavailable."""
 from ._lib import CudaFailure, CudaUnavailable, InvalidArgument, SimulatoError  # noqa: F401
 from .core import Antialias, AtomicStructure, ElectronBeam, Grid, Waves  # noqa: F401
 from .detector import (STEM, AnnularDetector, BinnedPixelatedDetector, CenterOfMassDetector,  # noqa: F401
-                       PixelatedDetector, ScanMeasurement, ScanWaves, SegmentedDetector, WavesDetector,
+                       PixelatedDetector, RealField, ScanMeasurement, ScanWaves, SegmentedDetector, WavesDetector,
                        detector_shape)
 from .engine import Engine, ExecutionOptions  # noqa: F401
 from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, JobTable,  # noqa: F401

@@ -34,7 +34,9 @@ EXPORTED = [
     "simk_scan_device", "simk_fft2", "simk_probe_spectrum_noalloc", "simk_finite_profile",
     "simk_potential_from_atoms_finite", "simk_surrogate_train", "simk_surrogate_destroy", "simk_surrogate_info",
     "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients", "simk_job_table_run",
-    "simk_scan_waves", "simk_ctf_kernel", "simk_apply_ctf",
+    "simk_scan_waves", "simk_ctf_kernel", "simk_apply_ctf", "simk_gaussian_source_size",
+    "simk_gaussian_source_size_device", "simk_poisson_noise", "simk_poisson_noise_device", "simk_integrate_gradient",
+    "simk_integrate_gradient_device",
 ]
 SURROGATE_PARAMS = 11249
 
@@ -136,6 +138,12 @@ def _signatures(lib):
         "simk_scan_waves": [P, C.POINTER(Probe_t), P, i32, PD, i32, i32, PD, PD],
         "simk_ctf_kernel": [P, C.POINTER(Grid_t), d, C.POINTER(Ctf_t), PD, PD],
         "simk_apply_ctf": [P, C.POINTER(Grid_t), d, C.POINTER(Ctf_t), i32, PD, PD, PD, PD, PD],
+        "simk_gaussian_source_size": [P, i32, i32, i64, d, d, d, d, PD, PD],
+        "simk_gaussian_source_size_device": [P, i32, i32, i64, d, d, d, d, P, P],
+        "simk_poisson_noise": [P, i64, PD, d, i32, C.c_uint64, PD],
+        "simk_poisson_noise_device": [P, i64, P, d, i32, C.c_uint64, P],
+        "simk_integrate_gradient": [P, i32, i32, d, d, PD, PD, i64, PD],
+        "simk_integrate_gradient_device": [P, i32, i32, d, d, P, P, i64, P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -5,6 +5,7 @@
 
 #include "context.cuh"
 #include "engine.cuh"
+#include "scanops.cuh"
 #include "surrogate.cuh"
 
 using namespace simk;
@@ -389,6 +390,106 @@ int simk_apply_ctf(simk_context* ctx, const simk_grid* grid, double energy, cons
         std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
         activate(ctx->impl);
         apply_ctf_device(ctx->impl, geom_of(grid), energy, *ctf, count, in_re, in_im, out_re, out_im, out_intensity);
+    });
+}
+
+// ---- scan post-processing ------------------------------------------------------------------------------------------
+
+int simk_gaussian_source_size_device(simk_context* ctx, int32_t nx, int32_t ny, int64_t value_count, double sigma_x,
+                                     double sigma_y, double sampling_x, double sampling_y, const double* in_device,
+                                     double* out_device) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && in_device && out_device, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        gaussian_source_size_device(ctx->impl, nx, ny, value_count, sigma_x, sigma_y, sampling_x, sampling_y,
+                                    in_device, out_device);
+    });
+}
+
+int simk_gaussian_source_size(simk_context* ctx, int32_t nx, int32_t ny, int64_t value_count, double sigma_x,
+                              double sigma_y, double sampling_x, double sampling_y, const double* in, double* out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && in && out, "null argument");
+        SIMK_REQUIRE(nx >= 1 && ny >= 1 && value_count >= 1, "the scan needs at least one position and one value");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        const size_t bytes = (size_t)nx * ny * value_count * sizeof(double);
+        DeviceBuffer d(bytes);
+        SIMK_CUDA(cudaMemcpyAsync(d.ptr, in, bytes, cudaMemcpyHostToDevice, c.stream));
+        gaussian_source_size_device(c, nx, ny, value_count, sigma_x, sigma_y, sampling_x, sampling_y, d.as<double>(),
+                                    d.as<double>());
+        SIMK_CUDA(cudaMemcpyAsync(out, d.ptr, bytes, cudaMemcpyDeviceToHost, c.stream));
+        SIMK_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int simk_poisson_noise_device(simk_context* ctx, int64_t count, const double* in_device, double dose, int32_t samples,
+                              uint64_t seed, double* out_device) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && (count == 0 || (in_device && out_device)), "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        poisson_noise_device(ctx->impl, count, in_device, dose, samples, seed, out_device);
+    });
+}
+
+int simk_poisson_noise(simk_context* ctx, int64_t count, const double* in, double dose, int32_t samples, uint64_t seed,
+                       double* out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && (count == 0 || (in && out)), "null argument");
+        SIMK_REQUIRE(count >= 0, "negative value count");
+        SIMK_REQUIRE(samples >= 1, "samples must be at least 1, got " + std::to_string(samples));
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        if (count == 0) {
+            poisson_noise_device(c, 0, nullptr, dose, samples, seed, nullptr);  // argument checks only
+            return;
+        }
+        DeviceBuffer din(count * sizeof(double)), dout((size_t)count * samples * sizeof(double));
+        SIMK_CUDA(cudaMemcpyAsync(din.ptr, in, count * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        poisson_noise_device(c, count, din.as<double>(), dose, samples, seed, dout.as<double>());
+        SIMK_CUDA(cudaMemcpyAsync(out, dout.ptr, (size_t)count * samples * sizeof(double), cudaMemcpyDeviceToHost,
+                                  c.stream));
+        SIMK_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int simk_integrate_gradient_device(simk_context* ctx, int32_t nx, int32_t ny, double sampling_x, double sampling_y,
+                                   const double* gx_device, const double* gy_device, int64_t stride,
+                                   double* out_device) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && gx_device && gy_device && out_device, "null argument");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        integrate_gradient_device(ctx->impl, nx, ny, sampling_x, sampling_y, gx_device, gy_device, stride, out_device);
+    });
+}
+
+int simk_integrate_gradient(simk_context* ctx, int32_t nx, int32_t ny, double sampling_x, double sampling_y,
+                            const double* gx, const double* gy, int64_t stride, double* out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && gx && gy && out, "null argument");
+        SIMK_REQUIRE(nx >= 2 && ny >= 2, "the gradient's images need at least 2 points per axis, got " +
+                                             std::to_string(nx) + " x " + std::to_string(ny));
+        SIMK_REQUIRE(stride >= 1, "the component stride must be at least 1");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        const long long n = (long long)nx * ny;
+        std::vector<double> h(2 * n);
+        for (long long i = 0; i < n; ++i) {
+            h[i] = gx[i * stride];
+            h[n + i] = gy[i * stride];
+        }
+        DeviceBuffer d(2 * n * sizeof(double)), o(n * sizeof(double));
+        SIMK_CUDA(cudaMemcpyAsync(d.ptr, h.data(), 2 * n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        integrate_gradient_device(c, nx, ny, sampling_x, sampling_y, d.as<double>(), d.as<double>() + n, 1,
+                                  o.as<double>());
+        SIMK_CUDA(cudaMemcpyAsync(out, o.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        SIMK_CUDA(cudaStreamSynchronize(c.stream));
     });
 }
 

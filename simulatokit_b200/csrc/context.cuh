@@ -143,6 +143,9 @@ struct Context {
     std::map<std::tuple<int, int, double, double, double, double, double, double>, std::unique_ptr<Propagator>> props;
     // workspaces
     DeviceBuffer work_a, work_b, work_c, rx, ry, positions, partial;
+    // scan post-processing: the Gaussian passes' intermediate, their weights, the Poisson sampler's status word, the
+    // gradient integration's two spectra and its minimum
+    DeviceBuffer post_work, post_weights, post_flag, post_spectra, post_min;
     std::vector<DeviceBuffer> outputs;
     // per-scan set-up kept across calls: detector maps by (grid, energy, detectors), spectra by (grid, probe)
     std::map<std::string, std::unique_ptr<DetectorPlan>> detector_plans;

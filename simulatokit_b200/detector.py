@@ -189,6 +189,122 @@ class ScanMeasurement:
     def array(self) -> np.ndarray:
         return self.values.reshape(tuple(self.scan_shape) + tuple(self.value_shape))
 
+    @property
+    def value_count(self) -> int:
+        return int(np.prod(self.value_shape)) if self.value_shape else 1
+
+    # ---- post-processing (ScanOperations.swift:12-117, IntegratedCenterOfMass.swift:11-41), on the device ----------
+
+    def gaussianSourceSize(self, sigma: float | None = None, *, sigmaX: float | None = None,
+                           sigmaY: float | None = None, samplingX: float, samplingY: float,
+                           engine: Engine | None = None) -> "ScanMeasurement":
+        """The scan with the finite source size of a Gaussian probe of standard deviation sigma [A] (or sigmaX,
+        sigmaY): every value filtered periodically over the scan with scipy's kernel, the scan's pixel sizes
+        samplingX, samplingY [A] (ScanOperations.swift:19-41). Bit-equal to the reference's float64 loop."""
+        if sigma is not None:
+            if sigmaX is not None or sigmaY is not None:
+                _refuse("give sigma or sigmaX and sigmaY, not both")
+            sigmaX = sigmaY = sigma
+        if sigmaX is None or sigmaY is None:
+            _refuse("give sigma or sigmaX and sigmaY")
+        for v in (sigmaX, sigmaY):
+            if not (math.isfinite(v) and v >= 0):
+                _refuse(f"the source size must be finite and non-negative, got ({sigmaX}, {sigmaY}) A")
+        for v in (samplingX, samplingY):
+            if not (math.isfinite(v) and v > 0):
+                _refuse(f"the scan sampling must be finite and positive, got ({samplingX}, {samplingY}) A")
+        if len(self.scan_shape) != 2:
+            _refuse("the source size filters a two-axis scan; a line scan has one axis")
+        e = engine or Engine.require()
+        vin = np.ascontiguousarray(self.values, dtype=np.float64).reshape(-1)
+        out = np.empty_like(vin)
+        L.check(e.lib.simk_gaussian_source_size(e.handle, self.scan_shape[0], self.scan_shape[1], self.value_count,
+                                                float(sigmaX), float(sigmaY), float(samplingX), float(samplingY),
+                                                L.dptr(vin), L.dptr(out)))
+        return ScanMeasurement(list(self.scan_shape), list(self.value_shape), out.reshape(np.shape(self.values)))
+
+    def poissonNoise(self, dose: float | None = None, *, dosePerArea: float | None = None,
+                     samplingX: float | None = None, samplingY: float | None = None, samples: int | None = None,
+                     seed: int = 0, engine: Engine | None = None):
+        """Poisson noise for a total dose [electrons per pattern] or a dose per area [electrons / A^2] over scan pixels
+        of samplingX x samplingY [A] (ScanOperations.swift:74-127): every value times the dose, clipped at 0, one
+        Poisson draw each. With `samples`, a list of that many independent draws. A seed gives the same noise on every
+        run; every value has a generator of its own (the reference's draws come from one stream)."""
+        if dosePerArea is not None:
+            if dose is not None:
+                _refuse("give dose or dosePerArea, not both")
+            for v in (samplingX, samplingY):
+                if v is None or not (math.isfinite(v) and v > 0):
+                    _refuse(f"the scan sampling must be finite and positive, got ({samplingX}, {samplingY}) A")
+            dose = samplingX * samplingY * dosePerArea
+        if dose is None:
+            _refuse("give dose or dosePerArea")
+        n_samples = 1 if samples is None else int(samples)
+        if n_samples < 1:
+            _refuse(f"samples must be at least 1, got {n_samples}")
+        vin = np.ascontiguousarray(self.values, dtype=np.float64).reshape(-1)
+        if n_samples * vin.size * 8 > _physical_memory_half():
+            _refuse(f"{n_samples} samples of {vin.size} values exceed half of the physical memory")
+        if not (math.isfinite(dose) and dose >= 0):
+            _refuse(f"the dose must be finite and non-negative, got {dose}")
+        e = engine or Engine.require()
+        out = np.empty(n_samples * vin.size)
+        L.check(e.lib.simk_poisson_noise(e.handle, vin.size, L.dptr(vin), float(dose), n_samples,
+                                         int(seed) & 0xFFFFFFFFFFFFFFFF, L.dptr(out)))
+        draws = [ScanMeasurement(list(self.scan_shape), list(self.value_shape),
+                                 out[s * vin.size:(s + 1) * vin.size].reshape(np.shape(self.values)))
+                 for s in range(n_samples)]
+        return draws if samples is not None else draws[0]
+
+    def gradientImages(self, samplingX: float, samplingY: float):
+        """The x and y components of a two-value (centre-of-mass) measurement as two images over the scan
+        (IntegratedCenterOfMass.swift:15-30)."""
+        if list(self.value_shape) != [2]:
+            _refuse(f"a centre-of-mass image needs two values per position (x, y), this measurement has shape "
+                    f"{self.value_shape}")
+        if len(self.scan_shape) != 2:
+            _refuse(f"a centre-of-mass image needs a two-axis scan, this measurement has scan shape {self.scan_shape}")
+        v = np.asarray(self.values, dtype=np.float64).reshape(self.scan_shape[0], self.scan_shape[1], 2)
+        nx, ny = self.scan_shape
+        return (RealField(nx, ny, v[..., 0].reshape(-1).copy(), samplingX, samplingY),
+                RealField(nx, ny, v[..., 1].reshape(-1).copy(), samplingX, samplingY))
+
+    def integratedCenterOfMass(self, samplingX: float, samplingY: float, engine: Engine | None = None) -> "RealField":
+        """The integrated centre of mass (IntegratedCenterOfMass.swift:36-40): the Fourier-space integral of the
+        centre-of-mass image, minimum 0, sampled as the scan."""
+        gx, gy = self.gradientImages(samplingX, samplingY)
+        return RealField.integratingGradient(gx, gy, engine=engine)
+
+
+@dataclass
+class RealField:
+    """A real nx x ny image, row-major [ix * ny + iy], with its pixel sizes [A] (SimulatoCore's RealField)."""
+    nx: int
+    ny: int
+    values: np.ndarray
+    samplingX: float
+    samplingY: float
+
+    @staticmethod
+    def integratingGradient(x: "RealField", y: "RealField", engine: Engine | None = None) -> "RealField":
+        """The integral of a gradient field (ImageOperations.swift:31-48, 140-167; abTEM integrate_gradient):
+        T^ = (kx g^x + ky g^y) / (2 pi i |k|^2), 0 at zero frequency, the real part of the inverse transform less its
+        minimum, on the device in float64."""
+        if (x.nx, x.ny, x.samplingX, x.samplingY) != (y.nx, y.ny, y.samplingX, y.samplingY):
+            _refuse("the two gradient components must have the same shape and sampling")
+        for v in (x.samplingX, x.samplingY):
+            if not (math.isfinite(v) and v > 0):
+                _refuse(f"invalid sampling ({x.samplingX}, {x.samplingY})")
+        if x.nx < 2 or x.ny < 2:
+            _refuse(f"the gradient's images need at least 2 points per axis, got {x.nx} x {x.ny}")
+        e = engine or Engine.require()
+        gx = np.ascontiguousarray(x.values, dtype=np.float64).reshape(-1)
+        gy = np.ascontiguousarray(y.values, dtype=np.float64).reshape(-1)
+        out = np.empty(x.nx * x.ny)
+        L.check(e.lib.simk_integrate_gradient(e.handle, x.nx, x.ny, float(x.samplingX), float(x.samplingY),
+                                              L.dptr(gx), L.dptr(gy), 1, L.dptr(out)))
+        return RealField(x.nx, x.ny, out, x.samplingX, x.samplingY)
+
 
 class STEM:
     """STEM.scan (STEM.swift:49-150) on the device."""

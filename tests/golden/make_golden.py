@@ -29,7 +29,8 @@ KEEP = {
     "slice-2": None,   # all (1.4 MB)
     "slice-4": None,
     "slice-3": None,   # CTF kernels and HRTEM images (1.5 MB)
-    "slice-4-scan": ["com_mrad", "com_inv", "dp"],
+    "slice-4-scan": ["com_mrad", "com_inv", "dp", "dp_gauss", "dp_gauss_big"],
+    "icom": None,      # gradient integrations, the scan's centre of mass and iCOM, disc and tile images (26 KB)
     "waves": None,     # all six runs (1.5 MB): full size and five Fourier resamplings
 }
 
