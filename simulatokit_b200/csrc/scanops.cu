@@ -47,7 +47,8 @@ __global__ void k_gauss_axis(const double* __restrict__ in, double* __restrict__
 // The same pass for axes whose element stride is at least 32 (a scan's values): a block takes 32 neighbouring columns
 // i0 .. i0 + 31 of one outer index and nk consecutive outputs k0 .. k0 + nk - 1 along the axis (the whole axis when it
 // fits, else windows of kTileOutputs), and stages rows k0 - r .. k0 + nk + r - 1 (indices mod L) in shared memory, one
-// coalesced 256-byte load per row; output k reads staged rows k - k0 + j, j < taps, with no index wrapping. Each
+// coalesced 256-byte asynchronous copy (cp.async) per row, into one of two buffers: the next tile's rows are in flight
+// while the current tile is computed. Output k reads staged rows k - k0 + j, j < taps, with no index wrapping. Each
 // warp computes kQ consecutive outputs per lane, the taps in chunks of kQ: a chunk's 2 kQ - 1 staged values and kQ
 // weights are loaded once into registers for kQ x kQ multiply-adds. Every output is still summed over j in order with
 // the same rounding as k_gauss_axis, so the two give identical bits.
@@ -55,42 +56,80 @@ constexpr int kWholeAxis = 256;
 constexpr int kTileOutputs = 64;
 constexpr int kQ = 8;
 constexpr int kMaxStagedRows = 384;                    // rows of real data
-constexpr int kStagedAlloc = kMaxStagedRows + 2 * kQ;  // plus the zero rows a ragged chunk may read: 100 KB
+constexpr int kStagedAlloc = kMaxStagedRows + 2 * kQ;  // plus the zero rows a ragged chunk may read
 
 __host__ __device__ inline int staged_outputs(int L, int radius) {
     return (L <= kWholeAxis && L + 2 * radius <= kMaxStagedRows) ? L : kTileOutputs;
 }
 
+struct AxisTile {
+    long long base;  // element (outer index, axis 0, this lane's column)
+    bool valid;      // this lane's column exists
+    int k0, nk, rows;
+};
+
+__device__ __forceinline__ AxisTile axis_tile(int t, int k_tiles, int col_tiles, int KT, int L, long long stride,
+                                              int radius, int lane) {
+    AxisTile a;
+    const int kt = t % k_tiles;
+    const int rest = t / k_tiles;
+    const int ct = rest % col_tiles;
+    const int o = rest / col_tiles;
+    const long long i = (long long)ct * 32 + lane;
+    a.valid = i < stride;
+    a.base = (long long)o * L * stride + i;
+    a.k0 = kt * KT;
+    a.nk = min(KT, L - a.k0);
+    a.rows = a.nk + 2 * radius;
+    return a;
+}
+
+// Staged row r of `buf` <- axis index (k0 - radius + r) mod L of this lane's column (asynchronously), zeros past the
+// tile's rows and for a missing column; each warp takes rows grp, grp + ngrp, ...
+__device__ __forceinline__ void stage_rows(double* buf, const double* __restrict__ in, const AxisTile& a, int L,
+                                           long long stride, int radius, int grp, int ngrp, int lane) {
+    int ax = ((a.k0 - radius + grp) % L + L) % L;
+    for (int r = grp; r < a.rows + 2 * kQ; r += ngrp) {
+        double* dst = buf + r * 32 + lane;
+        if (r < a.rows && a.valid) {
+            const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(in + a.base + (long long)ax * stride)
+                         : "memory");
+        } else {
+            *dst = 0.0;
+        }
+        ax += ngrp;
+        while (ax >= L) ax -= L;
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
 __global__ void k_gauss_axis_tiled(const double* __restrict__ in, double* __restrict__ out, int L, long long stride,
                                    int col_tiles, int tiles, const double* __restrict__ w, int taps, int radius) {
-    extern __shared__ double tile[];  // (rows + 2 kQ) x 32
+    extern __shared__ double staged[];  // two buffers of (KT + 2 radius + 2 kQ) x 32
     const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5, ngrp = blockDim.x >> 5;
     const int KT = staged_outputs(L, radius);
     const int k_tiles = (L + KT - 1) / KT;
     const int chunks = (taps + kQ - 1) / kQ;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int kt = t % k_tiles;
-        const int rest = t / k_tiles;
-        const int ct = rest % col_tiles;
-        const int o = rest / col_tiles;
-        const long long i = (long long)ct * 32 + lane;
-        const bool valid = i < stride;
-        const long long base = (long long)o * L * stride + i;
-        const int k0 = kt * KT;
-        const int nk = min(KT, L - k0);
-        const int rows = nk + 2 * radius;
-        __syncthreads();  // the previous tile's reads are done
-        // staged row r holds axis index (k0 - radius + r) mod L; each warp walks its rows r = grp, grp + ngrp, ...
-        int a = ((k0 - radius + grp) % L + L) % L;
-        for (int r = grp; r < rows + 2 * kQ; r += ngrp) {
-            double x = 0.0;
-            if (r < rows && valid) x = __ldg(in + base + (long long)a * stride);
-            tile[r * 32 + lane] = x;
-            a += ngrp;
-            while (a >= L) a -= L;
+    const int buf_rows = KT + 2 * radius + 2 * kQ;
+    int t = blockIdx.x;
+    if (t >= tiles) return;
+    AxisTile cur = axis_tile(t, k_tiles, col_tiles, KT, L, stride, radius, lane);
+    int which = 0;
+    stage_rows(staged, in, cur, L, stride, radius, grp, ngrp, lane);
+    for (; t < tiles; t += gridDim.x) {
+        const int tn = t + gridDim.x;
+        AxisTile next = cur;
+        if (tn < tiles) {
+            next = axis_tile(tn, k_tiles, col_tiles, KT, L, stride, radius, lane);
+            stage_rows(staged + (which ^ 1) * buf_rows * 32, in, next, L, stride, radius, grp, ngrp, lane);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
-        __syncthreads();
-        for (int kk0 = grp * kQ; kk0 < nk; kk0 += ngrp * kQ) {
+        __syncthreads();  // this tile's rows are in shared memory
+        const double* tile = staged + which * buf_rows * 32;
+        for (int kk0 = grp * kQ; kk0 < cur.nk; kk0 += ngrp * kQ) {
             double acc[kQ];
 #pragma unroll
             for (int q = 0; q < kQ; ++q) acc[q] = 0.0;
@@ -108,13 +147,16 @@ __global__ void k_gauss_axis_tiled(const double* __restrict__ in, double* __rest
                     }
                 }
             }
-            if (valid) {
-                double* o_ptr = out + base + (long long)(k0 + kk0) * stride;
+            if (cur.valid) {
+                double* o_ptr = out + cur.base + (long long)(cur.k0 + kk0) * stride;
 #pragma unroll
                 for (int q = 0; q < kQ; ++q)
-                    if (kk0 + q < nk) o_ptr[(long long)q * stride] = acc[q];
+                    if (kk0 + q < cur.nk) o_ptr[(long long)q * stride] = acc[q];
             }
         }
+        __syncthreads();  // this buffer's reads are done before the next-but-one tile is staged into it
+        cur = next;
+        which ^= 1;
     }
 }
 
@@ -303,6 +345,8 @@ void gaussian_source_size_device(Context& ctx, int nx, int ny, long long v, doub
                  "the scan sampling must be finite and positive, got (" + std::to_string(sampling_x) + ", " +
                      std::to_string(sampling_y) + ") A");
     SIMK_REQUIRE(nx >= 1 && ny >= 1 && v >= 1, "the scan needs at least one position and one value");
+    SIMK_REQUIRE((uintptr_t)in % sizeof(double) == 0 && (uintptr_t)out % sizeof(double) == 0,
+                 "the values must be 8-byte aligned float64 arrays");
     const long long total = (long long)nx * ny * v;
     struct AxisPass {
         int L;
@@ -352,7 +396,7 @@ void gaussian_source_size_device(Context& ctx, int nx, int ny, long long v, doub
                 static std::set<int> opted_in;  // devices whose launch limit was raised (under the context lock)
                 if (!opted_in.count(ctx.device)) {
                     SIMK_CUDA(cudaFuncSetAttribute(k_gauss_axis_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   kStagedAlloc * 32 * (int)sizeof(double)));
+                                                   2 * kStagedAlloc * 32 * (int)sizeof(double)));
                     opted_in.insert(ctx.device);
                 }
                 const long long outer = total / ((long long)L * stride);
@@ -360,7 +404,7 @@ void gaussian_source_size_device(Context& ctx, int nx, int ny, long long v, doub
                 const long long col_tiles = (stride + 31) / 32;
                 const long long tiles = outer * col_tiles * ((L + KT - 1) / KT);
                 SIMK_REQUIRE(tiles < (1LL << 31), "the scan's values are too many for one filter launch");
-                const size_t smem = (size_t)(rows + 2 * kQ) * 32 * sizeof(double);
+                const size_t smem = 2 * (size_t)(rows + 2 * kQ) * 32 * sizeof(double);  // two staging buffers
                 int per_sm = 0;
                 SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gauss_axis_tiled, 256, smem));
                 const long long resident = (long long)ctx.sm_count * std::max(1, per_sm);
