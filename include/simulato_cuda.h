@@ -152,6 +152,19 @@ int simk_potential_read_slices(simk_context* ctx, simk_potential* potential, dou
  * Multislice.swift:83-103), as stored on the device (complex64 widened). */
 int simk_potential_read_transmission(simk_context* ctx, simk_potential* potential, double energy, int32_t slice,
                                      double* re, double* im);
+/* ProjectedPotential.tiled(repetitionsX:repetitionsY:repetitionsZ:) (Sources/SimulatoMultislice/ProjectedPotential.swift:
+ * 76-105), on the device: `*out` is a new potential whose slices are `potential`'s tiled repetitions_x x repetitions_y
+ * times in the plane (extent multiplied, sampling kept), the whole stack repeated repetitions_z times. A periodic
+ * crystal built as one cell and tiled equals the crystal built atom by atom. Counts below 1, a tiled slice of more
+ * than 2^28 values, more than 1,000,000 slices or more than 2^31 values in all: SIMK_ERR_INVALID, before anything is
+ * allocated. Destroy the result with simk_potential_destroy. */
+int simk_potential_tile(simk_context* ctx, const simk_potential* potential, int32_t repetitions_x,
+                        int32_t repetitions_y, int32_t repetitions_z, simk_potential** out);
+/* ProjectedPotential.project() (ProjectedPotential.swift:64-73): the sum of the slices [V A], added in slice order in
+ * float64, into host out[nx ny]. */
+int simk_potential_project(simk_context* ctx, const simk_potential* potential, double* out);
+/* The grid a potential lives on (a tiled potential's is its source's times the repetitions). */
+int simk_potential_grid(const simk_potential* potential, simk_grid* grid);
 
 /* ---- finite projection and its learned surrogate -------------------------------------------------------------------
  * No reference implementation: SimulatoKit lists Potential(projection="finite") as not ported (docs/parity.md:58,251).

@@ -1256,3 +1256,44 @@ def poisson_noise_streams(values, dose: float, seed: int, samples: int = 1) -> n
             m = max(float(v[i]) * dose, 0.0)
             out[s, i] = float(poisson_draw(m, GaussianGenerator(poisson_value_seed(seed, s * n + i)))) if m > 0 else 0.0
     return out
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# Potential tiling, projection and crystal slicing (Sources/SimulatoMultislice/ProjectedPotential.swift:64-105,
+# Slicing.swift:43-69)
+# ---------------------------------------------------------------------------------------------------------------------
+
+def project_slices(values: np.ndarray) -> np.ndarray:
+    """ProjectedPotential.project: the slices [S][nx][ny] summed in order from 0."""
+    v = np.asarray(values, dtype=np.float64)
+    out = np.zeros(v.shape[1:])
+    for s in range(v.shape[0]):
+        out = out + v[s]
+    return out
+
+
+def tile_slices(values: np.ndarray, rx: int, ry: int, rz: int = 1) -> np.ndarray:
+    """ProjectedPotential.tiled: every slice tiled rx x ry in the plane, then the stack repeated rz times."""
+    v = np.asarray(values, dtype=np.float64)
+    return np.tile(v, (rz, rx, ry))
+
+
+def crystal_slice_thicknesses(z, depth: float, tolerance: float = 0.2):
+    """Slicing.crystalSliceThicknesses: the z of every atom with 0 and the depth, binned by floor(z / tolerance); the
+    differences between the occupied bins' centres (b + 1/2) tolerance. Raises ValueError where the reference throws."""
+    if not (math.isfinite(tolerance) and tolerance > 0):
+        raise ValueError("invalid tolerance")
+    bins = set()
+    for v in list(np.asarray(z, dtype=np.float64)) + [0.0, depth]:
+        q = float(v) / tolerance
+        if not (math.isfinite(q) and abs(math.floor(q)) <= 2.0 ** 53):
+            raise ValueError("invalid tolerance")
+        bins.add(math.floor(q))
+    centres = [(b + 0.5) * tolerance for b in sorted(bins)]
+    t = [c1 - c0 for c0, c1 in zip(centres, centres[1:])]
+    total = 0.0
+    for x in t:
+        total += x
+    if not t or abs(total - depth) > 1e-8 + 1e-5 * abs(depth):
+        raise ValueError("the thicknesses do not sum to the depth")
+    return t

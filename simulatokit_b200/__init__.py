@@ -13,5 +13,5 @@ from .detector import (STEM, AnnularDetector, BinnedPixelatedDetector, CenterOfM
 from .engine import Engine, ExecutionOptions  # noqa: F401
 from .multislice import (Backend, ExitPlanes, FrozenPhonons, GaussianGenerator, JobTable,  # noqa: F401
                          LobatoParameterization, Multislice, Potential, ProjectedPotential, Slicing, Surrogate,
-                         finite_profile)
+                         TiledPotential, finite_profile)
 from .probe import Aberrations, Aperture, ContrastTransferFunction, GridScan, Probe  # noqa: F401

@@ -36,7 +36,7 @@ EXPORTED = [
     "simk_surrogate_evaluate", "simk_surrogate_parameters", "simk_surrogate_gradients", "simk_job_table_run",
     "simk_scan_waves", "simk_ctf_kernel", "simk_apply_ctf", "simk_gaussian_source_size",
     "simk_gaussian_source_size_device", "simk_poisson_noise", "simk_poisson_noise_device", "simk_integrate_gradient",
-    "simk_integrate_gradient_device",
+    "simk_integrate_gradient_device", "simk_potential_tile", "simk_potential_project", "simk_potential_grid",
 ]
 SURROGATE_PARAMS = 11249
 
@@ -144,6 +144,9 @@ def _signatures(lib):
         "simk_poisson_noise_device": [P, i64, P, d, i32, C.c_uint64, P],
         "simk_integrate_gradient": [P, i32, i32, d, d, PD, PD, i64, PD],
         "simk_integrate_gradient_device": [P, i32, i32, d, d, P, P, i64, P],
+        "simk_potential_tile": [P, P, i32, i32, i32, C.POINTER(P)],
+        "simk_potential_project": [P, P, PD],
+        "simk_potential_grid": [P, C.POINTER(Grid_t)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

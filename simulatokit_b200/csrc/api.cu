@@ -5,6 +5,7 @@
 
 #include "context.cuh"
 #include "engine.cuh"
+#include "potops.cuh"
 #include "scanops.cuh"
 #include "surrogate.cuh"
 
@@ -280,6 +281,45 @@ int simk_potential_read_slices(simk_context* ctx, simk_potential* potential, dou
         SIMK_CUDA(cudaMemcpy(values, potential->impl.V.ptr,
                              (size_t)potential->impl.n_slices() * potential->impl.g.count() * sizeof(double),
                              cudaMemcpyDeviceToHost));
+    });
+}
+
+int simk_potential_tile(simk_context* ctx, const simk_potential* potential, int32_t repetitions_x,
+                        int32_t repetitions_y, int32_t repetitions_z, simk_potential** out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && potential && out, "null argument");
+        SIMK_REQUIRE(potential->impl.ctx == &ctx->impl, "the potential belongs to another context");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        auto p = std::make_unique<simk_potential>();
+        tile_potential(ctx->impl, potential->impl, repetitions_x, repetitions_y, repetitions_z, p->impl);
+        SIMK_CUDA(cudaStreamSynchronize(ctx->impl.stream));
+        *out = p.release();
+    });
+}
+
+int simk_potential_project(simk_context* ctx, const simk_potential* potential, double* out) {
+    return guarded([&] {
+        SIMK_REQUIRE(ctx && potential && out, "null argument");
+        SIMK_REQUIRE(potential->impl.ctx == &ctx->impl, "the potential belongs to another context");
+        std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+        activate(ctx->impl);
+        Context& c = ctx->impl;
+        const long long N = potential->impl.g.count();
+        DeviceBuffer d(N * sizeof(double));
+        project_potential(c, potential->impl, d.as<double>());
+        SIMK_CUDA(cudaMemcpyAsync(out, d.ptr, N * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        SIMK_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int simk_potential_grid(const simk_potential* potential, simk_grid* grid) {
+    return guarded([&] {
+        SIMK_REQUIRE(potential && grid, "null argument");
+        grid->nx = potential->impl.g.nx;
+        grid->ny = potential->impl.g.ny;
+        grid->extent_x = potential->impl.g.ex;
+        grid->extent_y = potential->impl.g.ey;
     });
 }
 

@@ -67,6 +67,30 @@ class Slicing:
         return lst
 
     @staticmethod
+    def crystalSliceThicknesses(structure: AtomicStructure, tolerance: float = 0.2):
+        """Slice thicknesses that follow the crystal planes (Slicing.swift:43-69, abTEM crystal_slice_thicknesses):
+        the z of every atom (as given) with 0 and the depth added, binned by floor(z / tolerance); the thicknesses are
+        the differences between the occupied bins' centres (b + 1/2) tolerance, in increasing z. Refused: a tolerance
+        that is not finite and positive (or z / tolerance past 2^53), and thicknesses that do not sum to the depth."""
+        if not (math.isfinite(tolerance) and tolerance > 0):
+            _refuse(f"invalid slice thickness {tolerance}")
+        depth = float(structure.box[2])
+        bins = set()
+        for z in list(np.asarray(structure.positions, dtype=np.float64)[:, 2]) + [0.0, depth]:
+            b = math.floor(float(z) / tolerance) if math.isfinite(float(z) / tolerance) else math.inf
+            if not (math.isfinite(b) and abs(b) <= 2.0 ** 53):
+                _refuse(f"invalid slice thickness {tolerance}")
+            bins.add(int(b))
+        centres = [(b + 0.5) * tolerance for b in sorted(bins)]
+        thicknesses = [c1 - c0 for c0, c1 in zip(centres, centres[1:])]
+        total = 0.0
+        for t in thicknesses:
+            total += t
+        if not thicknesses or abs(total - depth) > 1e-8 + 1e-5 * abs(depth):
+            _refuse(f"slice thicknesses sum to {total}, not the depth {depth}")
+        return thicknesses
+
+    @staticmethod
     def wrapped(s: AtomicStructure) -> np.ndarray:
         """Fractional mod 1 (ASE's wrap(eps=0)), z -> 0 within 1e-10 of the top face (Slicing.swift:71-84)."""
         p = s.positions.copy()
@@ -235,6 +259,85 @@ class Potential:
         v = self.handle(e).read_slices(self.slice_count, self.grid.nx, self.grid.ny)
         return ProjectedPotential(self.grid, v, self.slice_thicknesses)
 
+    def project(self, engine: Engine | None = None):
+        """Potential.project: the sum of the slices as an image (equal to build().project())."""
+        return _project(self, engine)
+
+    def tiled(self, repetitionsX: int, repetitionsY: int, repetitionsZ: int = 1) -> "TiledPotential":
+        """The built potential tiled on the device (ProjectedPotential.tiled, ProjectedPotential.swift:76-105)."""
+        return TiledPotential(self, repetitionsX, repetitionsY, repetitionsZ)
+
+
+def _project(p, engine):
+    """The sum of a potential's slices in slice order, on the device (ProjectedPotential.swift:64-73), as a RealField."""
+    from .detector import RealField
+    e = engine or Engine.require()
+    out = np.empty(p.grid.nx * p.grid.ny)
+    L.check(e.lib.simk_potential_project(e.handle, p.handle(e).handle, L.dptr(out)))
+    return RealField(p.grid.nx, p.grid.ny, out, p.grid.extent_x / p.grid.nx, p.grid.extent_y / p.grid.ny)
+
+
+def _check_repetitions(slices: int, nx: int, ny: int, rx, ry, rz):
+    """ProjectedPotential.tiled's refusals (ProjectedPotential.swift:82-92), all before any allocation: a count below
+    1 on any axis, more than 1,000,000 slices, a tiled slice of more than 2^28 values, more than 2^31 values in all."""
+    for r in (rx, ry, rz):
+        if isinstance(r, bool) or not isinstance(r, (int, np.integer)):
+            _refuse(f"repetitions must be integers, got ({rx}, {ry}, {rz})")
+    rx, ry, rz = int(rx), int(ry), int(rz)
+    per_slice = nx * rx * ny * ry
+    if (min(rx, ry, rz) < 1 or slices * rz > Slicing.maximum_slice_count or per_slice > 1 << 28
+            or per_slice * slices * rz > 1 << 31):
+        _refuse(f"repetitions must be at least 1 along both axes and give at most 2^28 values, got ({rx}, {ry})")
+    return rx, ry, rz
+
+
+class TiledPotential:
+    """A potential's slices tiled repetitionsX x repetitionsY times in the plane and the stack repeated repetitionsZ
+    times (ProjectedPotential.tiled, ProjectedPotential.swift:76-105; abTEM PotentialArray.tile): extent multiplied,
+    sampling kept. Built on the device from the source's device potential (simk_potential_tile) on first use, so a
+    periodic crystal costs one cell's build and a copy. Usable wherever a potential is."""
+
+    def __init__(self, source, repetitionsX: int, repetitionsY: int, repetitionsZ: int = 1):
+        g = source.grid
+        self.repetitions = _check_repetitions(source.slice_count, g.nx, g.ny, repetitionsX, repetitionsY,
+                                              repetitionsZ)
+        rx, ry, rz = self.repetitions
+        self.source = source
+        self.grid = Grid(g.nx * rx, g.ny * ry, g.extent_x * rx, g.extent_y * ry)
+        self.slice_thicknesses = list(source.slice_thicknesses) * rz
+        self.slice_of_atom = []
+        self._handles = {}
+
+    @property
+    def slice_count(self) -> int:
+        return len(self.slice_thicknesses)
+
+    @property
+    def thickness(self) -> float:
+        return float(sum(self.slice_thicknesses))
+
+    def handle(self, engine: Engine) -> PotentialHandle:
+        h = self._handles.get(id(engine))
+        if h is None:
+            out = C.c_void_p()
+            rx, ry, rz = self.repetitions
+            L.check(engine.lib.simk_potential_tile(engine.handle, self.source.handle(engine).handle, rx, ry, rz,
+                                                   C.byref(out)))
+            h = PotentialHandle(engine, out)
+            self._handles[id(engine)] = h
+        return h
+
+    def build(self, engine: Engine | None = None) -> "ProjectedPotential":
+        e = engine or Engine.require()
+        v = self.handle(e).read_slices(self.slice_count, self.grid.nx, self.grid.ny)
+        return ProjectedPotential(self.grid, v, self.slice_thicknesses)
+
+    def project(self, engine: Engine | None = None):
+        return _project(self, engine)
+
+    def tiled(self, repetitionsX: int, repetitionsY: int, repetitionsZ: int = 1) -> "TiledPotential":
+        return TiledPotential(self, repetitionsX, repetitionsY, repetitionsZ)
+
 
 class ProjectedPotential:
     """Slices of V [V A] on a grid (ProjectedPotential.swift:24-106)."""
@@ -263,6 +366,29 @@ class ProjectedPotential:
             h = PotentialHandle(engine, out)
             self._handles[id(engine)] = h
         return h
+
+    @property
+    def thickness(self) -> float:
+        return float(sum(self.slice_thicknesses))
+
+    def project(self, engine: Engine | None = None):
+        """ProjectedPotential.project (ProjectedPotential.swift:64-73): the slices summed in order, on the device; a
+        potential without slices projects to zeros."""
+        if self.slice_count == 0:
+            from .detector import RealField
+            g = self.grid
+            return RealField(g.nx, g.ny, np.zeros(g.nx * g.ny), g.extent_x / g.nx, g.extent_y / g.ny)
+        return _project(self, engine)
+
+    def tiled(self, repetitionsX: int, repetitionsY: int, repetitionsZ: int = 1):
+        """ProjectedPotential.tiled (ProjectedPotential.swift:76-105) on the device. A potential without slices tiles
+        to one without slices on the tiled grid (after the same refusals)."""
+        if self.slice_count == 0:
+            rx, ry, rz = _check_repetitions(0, self.grid.nx, self.grid.ny, repetitionsX, repetitionsY, repetitionsZ)
+            g = self.grid
+            return ProjectedPotential(Grid(g.nx * rx, g.ny * ry, g.extent_x * rx, g.extent_y * ry),
+                                      np.zeros((0, g.nx * rx, g.ny * ry)), [])
+        return TiledPotential(self, repetitionsX, repetitionsY, repetitionsZ)
 
 
 class ExitPlanes:
