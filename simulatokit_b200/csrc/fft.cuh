@@ -93,6 +93,78 @@ template <int DIR, typename V> __device__ __forceinline__ void bfly16(V* v) {
         v[k + 8] = e[k] - t;
     }
 }
+// ---- float32 butterflies on packed pairs ------------------------------------------------------------------------------
+// sm_100's add/sub/mul/fma.rn.f32x2 take a complex value as one 64-bit register pair, so a complex add is one
+// instruction instead of two. Multiplication by +-i becomes the swapped pair times (-+1, +-1) inside one packed FMA:
+// the products are exact, so every lane rounds as the scalar forms above do and the results are the same bits. These
+// overloads are more specialised than the templates above and serve every float2 butterfly of radix 2, 4 and 8.
+__device__ __forceinline__ unsigned long long pk(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 upk(unsigned long long r) {
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)), "l"(pk(c)));
+    return upk(r);
+}
+__device__ __forceinline__ float2 swp(float2 a) { return make_float2(a.y, a.x); }
+
+template <int DIR> __device__ __forceinline__ void bfly2(float2* v) {
+    const float2 a = v[0], b = v[1];
+    v[0] = padd(a, b);
+    v[1] = psub(a, b);
+}
+template <int DIR> __device__ __forceinline__ void bfly4(float2* v) {
+    const float2 a = padd(v[0], v[2]), b = psub(v[0], v[2]), c = padd(v[1], v[3]), e = psub(v[1], v[3]);
+    // d = (v1 - v3) i DIR = (-DIR e.y, DIR e.x): b +- d = (e.y, e.x) (-+DIR, +-DIR) + b
+    const float2 es = swp(e);
+    v[0] = padd(a, c);
+    v[2] = psub(a, c);
+    v[1] = pfma(es, make_float2((float)-DIR, (float)DIR), b);
+    v[3] = pfma(es, make_float2((float)DIR, (float)-DIR), b);
+}
+template <int DIR> __device__ __forceinline__ void bfly8(float2* v) {
+    const float c = 0.70710678118654752440f;
+    float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    bfly4<DIR>(e);
+    bfly4<DIR>(o);
+    // o1 = ((o.x - DIR o.y) c, (o.y + DIR o.x) c); o3 = ((-o.x - DIR o.y) c, (-o.y + DIR o.x) c)
+    //    = ((o.x + DIR o.y) (-c), (o.y - DIR o.x) (-c))
+    const float2 o1 = pmul(pfma(swp(o[1]), make_float2((float)-DIR, (float)DIR), o[1]), make_float2(c, c));
+    const float2 o3 = pmul(pfma(swp(o[3]), make_float2((float)DIR, (float)-DIR), o[3]), make_float2(-c, -c));
+    v[0] = padd(e[0], o[0]);
+    v[4] = psub(e[0], o[0]);
+    v[1] = padd(e[1], o1);
+    v[5] = psub(e[1], o1);
+    // e2 +- o2, o2 = o[2] i DIR
+    const float2 s2 = swp(o[2]);
+    v[2] = pfma(s2, make_float2((float)-DIR, (float)DIR), e[2]);
+    v[6] = pfma(s2, make_float2((float)DIR, (float)-DIR), e[2]);
+    v[3] = padd(e[3], o3);
+    v[7] = psub(e[3], o3);
+}
+
 // The p-point DFT by its definition, for odd prime radices (7, 11, ...): W_p^{rq} from a table of cos/sin(2 pi k/p).
 template <int DIR, typename V>
 __device__ __forceinline__ void dft_direct(V* v, int R, const double* ctab, const double* stab) {
