@@ -446,6 +446,8 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
         float2* dst = stages + s * 2 * TILE;
         const int prow = p_row ? p_row[b] * N : 0;  // job tables: this wave's propagator among the stacked ones
+        // ENG 0 stores each tile from its stage with TMA: the previous tile's store must have read the stage first
+        if constexpr (ENG == 0) bulk_wait_read();
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
 #pragma unroll
         for (int k = 0; k < NBOX; ++k) {
@@ -465,7 +467,12 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             stage_wait(full, s, it, next < ntiles, err, &abort_flag);
         }
         __syncthreads();
-        if (abort_flag) return;
+        if (abort_flag) {
+            if constexpr (ENG == 0) {
+                if (tid == 0) bulk_wait_all();
+            }
+            return;
+        }
         const int b = (int)(tile / tiles_per_wave);
         const int iy = (int)(tile - (unsigned)b * tiles_per_wave) * TC + c;
         float2* col = psi + (size_t)b * N * ny + iy;
@@ -479,8 +486,10 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
 #pragma unroll
             for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], pbuf[(t + T * i) * TC + c]) * pscale;
             if constexpr (MODE == 0) ct_fft_from<N, 0, +1>(v, t, eng, sm);
+            // back into the stage tile in its natural [row][TC] layout (every exchange read is behind a barrier);
+            // thread 0 stores the tile with TMA after the barrier below
 #pragma unroll
-            for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
+            for (int i = 0; i < 8; ++i) buf[(t + T * i) * TC + c] = v[i];
         } else if constexpr (ENG == 2) {
             using L = CcLayout<N, TC, true>;
             float2* scratch = stages + 4 * TILE;
@@ -512,6 +521,18 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         }
         fence_proxy_async_shared();
         __syncthreads();  // every thread is done with the stage before its next copy
+        if constexpr (ENG == 0) {
+            if (tid == 0) {
+                const int b = (int)(tile / tiles_per_wave);
+                const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
+#pragma unroll
+                for (int k = 0; k < NBOX; ++k) tma_store_2d(&map, buf + k * BOXH * TC, 2 * iy0, b * N + k * BOXH);
+                bulk_commit();
+            }
+        }
+    }
+    if constexpr (ENG == 0) {
+        if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
     }
 }
 
@@ -547,6 +568,8 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
     auto issue = [&](int tile, int s) {
         float2* dst = stages + s * 2 * TILE;
         const int row0 = tile * RB;
+        // ENG 0 stores each tile from its stage: the previous tile's store must have read the stage first
+        if constexpr (ENG == 0) bulk_wait_read();
         mbar_arrive_expect_tx(&full[s], with_t ? 2 * bytes : bytes);
         bulk_load(dst, psi + (size_t)row0 * N, bytes, &full[s]);
         if (with_t) {
@@ -566,7 +589,12 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
             stage_wait(full, s, it, next < ntiles, err, &abort_flag);
         }
         __syncthreads();
-        if (abort_flag) return;
+        if (abort_flag) {
+            if constexpr (ENG == 0) {
+                if (tid == 0) bulk_wait_all();
+            }
+            return;
+        }
         float2* row = psi + (size_t)(tile * RB + rr) * N;
         if constexpr (ENG == 0) {
             float2 v[8];
@@ -583,8 +611,10 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
                 for (int i = 0; i < 8; ++i) v[i] = v[i] * scale;
             }
             if (fwd) ct_fft_from<N, 0, -1>(v, t, eng, sm);
+            // back into the stage rows (every exchange read is behind a barrier); thread 0 stores them after the
+            // barrier below
 #pragma unroll
-            for (int i = 0; i < 8; ++i) row[t + T * i] = v[i];
+            for (int i = 0; i < 8; ++i) buf[rr * N + t + T * i] = v[i];
         } else if constexpr (ENG == 2) {
             using L = CcLayout<N, RB, false>;
             float2* scratch = stages + 4 * TILE;
@@ -633,7 +663,16 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
             }
         }
         fence_proxy_async_shared();
-        __syncthreads();
+        __syncthreads();  // every thread is done with the stage before its next copy
+        if constexpr (ENG == 0) {
+            if (tid == 0) {
+                bulk_store(psi + (size_t)tile * RB * N, buf, bytes);
+                bulk_commit();
+            }
+        }
+    }
+    if constexpr (ENG == 0) {
+        if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
     }
 }
 

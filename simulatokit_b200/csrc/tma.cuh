@@ -1,5 +1,5 @@
 // tma.cuh -- Blackwell/Hopper asynchronous copies for the fused passes: mbarriers, bounded waits, 2-D tiled TMA loads
-// (cp.async.bulk.tensor, no multicast) and the host-side tensor-map encoding through the driver entry point.
+// and stores (cp.async.bulk.tensor, no multicast) and the host-side tensor-map encoding through the driver entry point.
 #pragma once
 
 #include <cuda.h>
@@ -62,6 +62,26 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+
+// One 2-D tiled TMA store of the box at (x, y) from shared memory, in the issuing thread's bulk async-group. x as for
+// tma_load_2d. The shared-memory source must not be rewritten until bulk_wait_read() says the copy has read it.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(x),
+                 "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+// One contiguous bulk copy shared -> global of `bytes` (a multiple of 16; both addresses 16-byte aligned), in the
+// issuing thread's bulk async-group.
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Until every bulk store this thread committed has read its shared-memory source.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Until every bulk store this thread committed is complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // Encodes a 2-D float32 tensor map over a row-major array of `rows` rows of `inner` floats, box = box_inner floats x
 // box_rows rows, no swizzle, no interleave.
