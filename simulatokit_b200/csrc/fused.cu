@@ -446,8 +446,6 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
         float2* dst = stages + s * 2 * TILE;
         const int prow = p_row ? p_row[b] * N : 0;  // job tables: this wave's propagator among the stacked ones
-        // ENG 0 stores each tile from its stage with TMA: the previous tile's store must have read the stage first
-        if constexpr (ENG == 0) bulk_wait_read();
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
 #pragma unroll
         for (int k = 0; k < NBOX; ++k) {
@@ -463,19 +461,20 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         const float2* pbuf = buf + TILE;
         const unsigned next = tile + gridDim.x;
         if (tid == 0) {
+            // the previous tile's TMA store must have read its shared-memory source (a stage or the scratch tile)
+            // before the next copy into a stage and before this tile's transforms write the scratch tile
+            bulk_wait_read();
             if (next < ntiles) issue(next, s ^ 1);
             stage_wait(full, s, it, next < ntiles, err, &abort_flag);
         }
         __syncthreads();
         if (abort_flag) {
-            if constexpr (ENG == 0) {
-                if (tid == 0) bulk_wait_all();
-            }
+            if (tid == 0) bulk_wait_all();
             return;
         }
         const int b = (int)(tile / tiles_per_wave);
         const int iy = (int)(tile - (unsigned)b * tiles_per_wave) * TC + c;
-        float2* col = psi + (size_t)b * N * ny + iy;
+        const float2* store_src = buf;  // where the finished tile lies in its natural layout
         if constexpr (ENG == 0) {
             float2 v[8];
 #pragma unroll
@@ -490,6 +489,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             // thread 0 stores the tile with TMA after the barrier below
 #pragma unroll
             for (int i = 0; i < 8; ++i) buf[(t + T * i) * TC + c] = v[i];
+            store_src = buf;
         } else if constexpr (ENG == 2) {
             using L = CcLayout<N, TC, true>;
             float2* scratch = stages + 4 * TILE;
@@ -498,12 +498,16 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
                 float2* other = (out == buf) ? scratch : buf;
                 out = cc_fft<N, TC, true, +1, PRE_MUL, false>(out, other, pbuf, pscale, tw, tid);
             }
+            float2 v[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                float2 v = out[L::at(c, (int)t + T * i)];
-                if constexpr (MODE == 1) v = cmul(v, pbuf[L::nat(c, (int)t + T * i)]) * pscale;
-                col[(size_t)(t + T * i) * ny] = v;
+                v[i] = out[L::at(c, (int)t + T * i)];
+                if constexpr (MODE == 1) v[i] = cmul(v[i], pbuf[L::nat(c, (int)t + T * i)]) * pscale;
             }
+            __syncthreads();  // every thread has read `out`: it takes the tile in its natural [row][TC] layout
+#pragma unroll
+            for (int i = 0; i < 8; ++i) out[(t + T * i) * TC + c] = v[i];
+            store_src = out;
         } else {
             using L = TileLayout<N, TC, true>;
             float2* scratch = stages + 4 * TILE;
@@ -512,28 +516,27 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
                 float2* other = (out == buf) ? scratch : buf;
                 out = tc_fft<N, TC, true, +1, PRE_MUL, false>(out, other, pbuf, pscale, tw, eng, tid);
             }
+            float2 v[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                float2 v = out[L::at(c, (int)t + T * i)];
-                if constexpr (MODE == 1) v = cmul(v, pbuf[L::nat(c, (int)t + T * i)]) * pscale;
-                col[(size_t)(t + T * i) * ny] = v;
+                v[i] = out[L::at(c, (int)t + T * i)];
+                if constexpr (MODE == 1) v[i] = cmul(v[i], pbuf[L::nat(c, (int)t + T * i)]) * pscale;
             }
+            __syncthreads();  // every thread has read `out`: it takes the tile in its natural [row][TC] layout
+#pragma unroll
+            for (int i = 0; i < 8; ++i) out[(t + T * i) * TC + c] = v[i];
+            store_src = out;
         }
         fence_proxy_async_shared();
         __syncthreads();  // every thread is done with the stage before its next copy
-        if constexpr (ENG == 0) {
-            if (tid == 0) {
-                const int b = (int)(tile / tiles_per_wave);
-                const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
+        if (tid == 0) {
+            const int iy0 = iy - c;
 #pragma unroll
-                for (int k = 0; k < NBOX; ++k) tma_store_2d(&map, buf + k * BOXH * TC, 2 * iy0, b * N + k * BOXH);
-                bulk_commit();
-            }
+            for (int k = 0; k < NBOX; ++k) tma_store_2d(&map, store_src + k * BOXH * TC, 2 * iy0, b * N + k * BOXH);
+            bulk_commit();
         }
     }
-    if constexpr (ENG == 0) {
-        if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
-    }
+    if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
 }
 
 // rows: tile = RB consecutive rows of one wave (nx % RB == 0); a stage holds those RB rows and the RB rows of t.
