@@ -208,24 +208,22 @@ def sample_indices(n_positions: int):
 def cpu_reference(n_positions: int, threads: int, want_values: bool = False):
     """Times the C++ float64 restatement of STEM.cpuScan (oracle/cpu/simk_cpu.cpp: FFT2D's mixed-radix / Bluestein
     transforms, runCPU, Probe.build, the annular detectors) on `n_positions` positions of the workload, `threads`
-    workers over positions as runCPUParallel. The transmissions, propagators, probe spectrum and masks are built once
-    beforehand (float64 NumPy oracle), as runBatch shares them. Returns (steps/s, seconds, positions) and, with
-    want_values, the detector values at those positions ([detector][position])."""
+    workers over positions as runCPUParallel. The potential, transmissions, propagators, probe spectrum and masks are
+    built once beforehand by the same C++ restatement, as runBatch shares them. Returns (steps/s, seconds, positions)
+    and, with want_values, the detector values at those positions ([detector][position])."""
     from oracle import simk_cpu as K
     from oracle import simk_oracle as O
     box, nums, pos = srtio3(8, 8, 20)
     s = O.Structure(box, nums, pos)
-    p = O.Potential.from_structure(s, NX, NY, slice_thickness=SLICE, pi_choice="exact")
-    g = p.grid
-    ts = [O.transmission(v, ENERGY, g) for v in p.build()]
     spec = O.ProbeSpec(ENERGY, SEMIANGLE)
-    inputs = K.ScanInputs(spec, g, ts, p.thicknesses, K.annular_masks(g, ENERGY, [(a, b) for _, a, b in DETECTORS]))
+    thicknesses = O.slice_thicknesses(box[2], SLICE)
+    inputs = K.ScanInputs.from_structure(spec, s, NX, NY, thicknesses, [(a, b) for _, a, b in DETECTORS])
     positions = scan_positions()[sample_indices(n_positions)]
     inputs.scan(positions[:1], threads=1)  # warm-up
     t0 = time.perf_counter()
     vals = inputs.scan(positions, threads=threads)
     dt = time.perf_counter() - t0
-    out = (len(positions) * len(p.thicknesses) / dt, dt, len(positions))
+    out = (len(positions) * len(thicknesses) / dt, dt, len(positions))
     if want_values:
         return out + ([vals[:, d].copy() for d in range(len(DETECTORS))],)
     return out

@@ -461,7 +461,8 @@ struct Work2 {
 
 // In place on the split field (re, im: nx ny, row-major [ix][iy]), rows then columns. Optional elementwise factors:
 // `pre` multiplies the field before the transform (fused into the row gather) and `post` after it (fused into the
-// column scatter); `scale` multiplies the result. sign -1: NumPy's fft2; +1 with scale 1 / (nx ny): its ifft2.
+// column scatter); a null imaginary part makes a factor real. `scale` multiplies the result. sign -1: NumPy's fft2;
+// +1 with scale 1 / (nx ny): its ifft2.
 void fft2(const Plan2& p, double* re, double* im, int sign, Work2& ws, const double* pre_r = nullptr,
           const double* pre_i = nullptr, const double* post_r = nullptr, const double* post_i = nullptr,
           double scale = 1.0) {
@@ -481,7 +482,13 @@ void fft2(const Plan2& p, double* re, double* im, int sign, Work2& ws, const dou
                 const size_t base = (size_t)(x0 + l) * ny;
                 const double* a = re + base;
                 const double* b = im + base;
-                if (pre_r) {
+                if (pre_r && !pre_i) {
+                    const double* c = pre_r + base;
+                    for (int y = 0; y < ny; ++y) {
+                        lr[(size_t)y * B + l] = a[y] * c[y];
+                        li[(size_t)y * B + l] = b[y] * c[y];
+                    }
+                } else if (pre_r) {
                     const double* c = pre_r + base;
                     const double* d = pre_i + base;
                     for (int y = 0; y < ny; ++y) {
@@ -525,7 +532,7 @@ void fft2(const Plan2& p, double* re, double* im, int sign, Work2& ws, const dou
             for (int l = 0; l < cnt; ++l) {
                 double vr = lr[(size_t)x * B + l], vi = li[(size_t)x * B + l];
                 if (post_r) {
-                    const double c = post_r[base + l], d = post_i[base + l];
+                    const double c = post_r[base + l], d = post_i ? post_i[base + l] : 0.0;
                     const double tr = vr * c - vi * d;
                     vi = vr * d + vi * c;
                     vr = tr;
@@ -535,6 +542,79 @@ void fft2(const Plan2& p, double* re, double* im, int sign, Work2& ws, const dou
             }
         }
     }
+}
+
+// ---- the per-potential set-up of the scan, restated (each stage follows the float64 NumPy oracle's order) ------------
+
+constexpr double kPlanck = 6.62607004e-34, kMass = 9.10938356e-31, kLight = 299792458.0,
+                 kCharge = 1.6021766208e-19, kKappa = 0.0208865737082965, kAseKg = 6.0221408585491615e26,
+                 kAseCoulomb = 6.241509125883258e18, kAseSecond = 98226947884640.62,
+                 kAseJoule = 6.241509125883258e18;
+
+// ElectronBeam.swift:38-43 and 24-30
+double wavelength(double e) {
+    const double c2 = kLight * kLight;
+    return kPlanck * kLight / std::sqrt(e * (2 * kMass * c2 / kCharge + e)) / kCharge * 1.0e10;
+}
+double interaction_parameter(double e) {
+    const double mass = (1 + kCharge * e / (kMass * (kLight * kLight))) * kMass;
+    const double hsj = kPlanck * kAseSecond * kAseJoule;
+    return 2 * M_PI * mass * kAseKg * kCharge * kAseCoulomb * wavelength(e) / (hsj * hsj);
+}
+
+// Grid.swift:45-86: sampling extent / n, NumPy's fftfreq(n, d) bit for bit.
+struct Geo {
+    int nx, ny;
+    double ex, ey;
+    double dx() const { return ex / nx; }
+    double dy() const { return ey / ny; }
+    size_t count() const { return (size_t)nx * ny; }
+};
+std::vector<double> fftfreq(int n, double d) {
+    const double val = 1.0 / (n * d);
+    const int pos = (n - 1) / 2 + 1;
+    std::vector<double> f(n);
+    for (int i = 0; i < n; ++i) f[i] = (double)(i < pos ? i : i - n) * val;
+    return f;
+}
+
+// Antialias.swift:18-52
+std::vector<double> antialias(const Geo& g) {
+    const double dmax = std::max(g.dx(), g.dy());
+    const double kc = 0.6666666 / dmax / 2, w = 0.01 / dmax;
+    const std::vector<double> kx = fftfreq(g.nx, g.dx()), ky = fftfreq(g.ny, g.dy());
+    std::vector<double> out(g.count(), 1.0);
+    for (int ix = 0; ix < g.nx; ++ix)
+        for (int iy = 0; iy < g.ny; ++iy) {
+            const double r = std::sqrt(kx[ix] * kx[ix] + ky[iy] * ky[iy]);
+            double& o = out[(size_t)ix * g.ny + iy];
+            if (r > kc - w && r <= kc) o = 0.5 * (1 + std::cos(M_PI * (r - kc + w) / w));
+            if (r > kc) o = 0.0;
+        }
+    return out;
+}
+
+// Aberrations.swift:39-59 with NumPy's grouping; ab in simk_probe's order (C10 C12 phi12 C21 phi21 C23 phi23 C30 C32
+// phi32 C34 phi34 C41 phi41 C43 phi43 C45 phi45 C50 C52 phi52 C54 phi54 C56 phi56).
+double chi(double alpha, double phi, const double* ab, double lam) {
+    enum { C10, C12, P12, C21, P21, C23, P23, C30, C32, P32, C34, P34, C41, P41, C43, P43, C45, P45, C50, C52, P52,
+           C54, P54, C56, P56 };
+    double x = 0.0;
+    if (ab[C10] || ab[C12] || ab[P12]) x = x + 1.0 / 2 * std::pow(alpha, 2) * (ab[C10] + ab[C12] * std::cos(2 * (phi - ab[P12])));
+    if (ab[C21] || ab[P21] || ab[C23] || ab[P23])
+        x = x + 1.0 / 3 * std::pow(alpha, 3) * (ab[C21] * std::cos(phi - ab[P21]) + ab[C23] * std::cos(3 * (phi - ab[P23])));
+    if (ab[C30] || ab[C32] || ab[P32] || ab[C34] || ab[P34])
+        x = x + 1.0 / 4 * std::pow(alpha, 4) *
+                    (ab[C30] + ab[C32] * std::cos(2 * (phi - ab[P32])) + ab[C34] * std::cos(4 * (phi - ab[P34])));
+    if (ab[C41] || ab[P41] || ab[C43] || ab[P43] || ab[C45] || ab[P45])
+        x = x + 1.0 / 5 * std::pow(alpha, 5) *
+                    (ab[C41] * std::cos(phi - ab[P41]) + ab[C43] * std::cos(3 * (phi - ab[P43])) +
+                     ab[C45] * std::cos(5 * (phi - ab[P45])));
+    if (ab[C50] || ab[C52] || ab[P52] || ab[C54] || ab[P54] || ab[C56] || ab[P56])
+        x = x + 1.0 / 6 * std::pow(alpha, 6) *
+                    (ab[C50] + ab[C52] * std::cos(2 * (phi - ab[P52])) + ab[C54] * std::cos(4 * (phi - ab[P54])) +
+                     ab[C56] * std::cos(6 * (phi - ab[P56])));
+    return x * (2 * M_PI / lam);
 }
 
 }  // namespace
@@ -632,6 +712,258 @@ int simk_cpu_stem_scan(int nx, int ny, int n_slices, const double* t_re, const d
     for (int t = 1; t < T; ++t) pool.emplace_back(work, t, T);
     work(0, T);
     for (auto& th : pool) th.join();
+    return 0;
+}
+
+// ---- the per-potential set-up ----------------------------------------------------------------------------------------
+
+// The infinite-projection Lobato potential (ProjectedPotential.swift:110-201, Slicing.swift:71-104): atoms wrapped into
+// the box (top-face rule), sliced at the nudged cumulative edges, then per slice and per element in increasing Z the
+// bilinear deltas (weights added atom by atom), FFT2, times f(k^2) / S(k), inverse FFT2, real part, summed. Lobato
+// parameters: n_table elements, table_z[e] with a[5 e .. 5 e + 4], b[..]; pi_choice 0 exact, 1 abTEM's float32 pi.
+// out: n_slices x nx x ny V [V A]. Returns 1 for bad arguments, 2 for an element missing from the table.
+int simk_cpu_potential(int nx, int ny, double ex, double ey, double ez, int n_slices, const double* thickness,
+                       int n_atoms, const int* z, const double* xyz, int n_table, const int* table_z,
+                       const double* table_a, const double* table_b, int pi_choice, double* out) {
+    if (nx < 1 || ny < 1 || n_slices < 1 || n_atoms < 0 || !(ex > 0 && ey > 0 && ez > 0)) return 1;
+    const Geo g{nx, ny, ex, ey};
+    const size_t N = g.count();
+    // wrap (fractional mod 1, ASE's wrap(eps=0)) and the top-face rule
+    std::vector<double> p((size_t)n_atoms * 3);
+    const double box[3] = {ex, ey, ez};
+    for (int a = 0; a < n_atoms; ++a) {
+        for (int d = 0; d < 3; ++d) {
+            double f = std::fmod(xyz[3 * a + d] / box[d], 1.0);
+            if (f < 0) f += 1.0;
+            if (f == 1.0) f = 0.0;
+            p[3 * a + d] = f * box[d];
+        }
+        if (p[3 * a + 2] > ez - 1e-10) p[3 * a + 2] = 0.0;
+    }
+    // slice of each atom: first edge strictly greater than z, edges = running sums - 1e-12; the last slice at most
+    std::vector<double> edges(n_slices);
+    double acc = 0.0;
+    for (int j = 0; j < n_slices; ++j) {
+        acc += thickness[j];
+        edges[j] = acc - 1e-12;
+    }
+    std::vector<int> slice_of(n_atoms);
+    for (int a = 0; a < n_atoms; ++a) {
+        const int k = (int)(std::upper_bound(edges.begin(), edges.end(), p[3 * a + 2]) - edges.begin());
+        slice_of[a] = std::min(k, n_slices - 1);
+    }
+    // kernels f(k^2) / S(k) per element present
+    const std::vector<double> kx = fftfreq(nx, g.dx()), ky = fftfreq(ny, g.dy());
+    std::vector<double> k2(N), comp(N);
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            const size_t i = (size_t)ix * ny + iy;
+            k2[i] = kx[ix] * kx[ix] + ky[iy] * ky[iy];
+            const double a = kx[ix] * g.dx(), b = ky[iy] * g.dy();
+            const double k = (ix == 0 && iy == 0) ? 1.0 : std::sqrt(a * a + b * b);
+            comp[i] = (ix == 0 && iy == 0) ? g.dx() * g.dy() : std::sin(k) / k * (g.dx() * g.dy());
+        }
+    const double pi = pi_choice ? (double)(float)M_PI : M_PI;
+    const double pi2 = pi_choice ? (double)(float)(M_PI * M_PI) : M_PI * M_PI;
+    std::vector<int> elements(z, z + n_atoms);
+    std::sort(elements.begin(), elements.end());
+    elements.erase(std::unique(elements.begin(), elements.end()), elements.end());
+    std::vector<std::vector<double>> kernel(elements.size());
+    for (size_t e = 0; e < elements.size(); ++e) {
+        int row = -1;
+        for (int t = 0; t < n_table; ++t)
+            if (table_z[t] == elements[e]) row = t;
+        if (row < 0) return 2;
+        double A[5], B[5];
+        for (int i = 0; i < 5; ++i) {
+            const double a = table_a[5 * row + i], b = table_b[5 * row + i];
+            A[i] = M_PI * M_PI * a / std::pow(b, 1.5) / kKappa;
+            B[i] = 2 * M_PI / std::sqrt(b);
+        }
+        kernel[e].resize(N);
+        for (size_t i = 0; i < N; ++i) {
+            const double q = (4 * pi2) * k2[i];
+            double sum = 0.0;
+            for (int t = 0; t < 5; ++t) {
+                const double d = q + B[t] * B[t];
+                sum = sum + (A[t] / B[t] / d + A[t] * B[t] / (d * d));
+            }
+            kernel[e][i] = (8 * pi) * sum / comp[i];
+        }
+    }
+    const Plan2 plan = make_plan2(nx, ny);
+    Work2 ws;
+    std::vector<double> dr(N), di(N);
+    for (int j = 0; j < n_slices; ++j) {
+        double* v = out + (size_t)j * N;
+        std::fill(v, v + N, 0.0);
+        for (size_t e = 0; e < elements.size(); ++e) {
+            std::fill(dr.begin(), dr.end(), 0.0);
+            std::fill(di.begin(), di.end(), 0.0);
+            bool any = false;
+            // weights in NumPy's np.add.at order: weight k outer, atoms inner
+            for (int k = 0; k < 4; ++k)
+                for (int a = 0; a < n_atoms; ++a) {
+                    if (slice_of[a] != j || z[a] != elements[e]) continue;
+                    any = true;
+                    const double px = p[3 * a] / g.dx(), py = p[3 * a + 1] / g.dy();
+                    const double rf = std::floor(px), cf = std::floor(py);
+                    const double x = px - rf, y = py - cf, xy = x * y;
+                    const double w[4] = {1 + xy - y - x, x - xy, y - xy, xy};
+                    long long r = (long long)rf + ((k == 1 || k == 3) ? 1 : 0);
+                    long long c = (long long)cf + (k >= 2 ? 1 : 0);
+                    r %= nx;
+                    if (r < 0) r += nx;
+                    c %= ny;
+                    if (c < 0) c += ny;
+                    dr[(size_t)r * ny + c] += w[k];
+                }
+            if (!any) continue;
+            fft2(plan, dr.data(), di.data(), -1, ws, nullptr, nullptr, kernel[e].data(), nullptr);
+            fft2(plan, dr.data(), di.data(), +1, ws, nullptr, nullptr, nullptr, nullptr, 1.0 / (double)N);
+            for (size_t i = 0; i < N; ++i) v[i] = v[i] + dr[i];
+        }
+    }
+    return 0;
+}
+// The band-limited transmission of one slice (Multislice.swift:83-103): t = IFFT2(FFT2(e^{i sigma V}) A).
+int simk_cpu_transmission(int nx, int ny, double ex, double ey, double energy, const double* v, double* re,
+                          double* im) {
+    if (nx < 1 || ny < 1 || !(ex > 0 && ey > 0 && energy > 0)) return 1;
+    const Geo g{nx, ny, ex, ey};
+    const size_t N = g.count();
+    const double sigma = interaction_parameter(energy);
+    for (size_t i = 0; i < N; ++i) {
+        const double x = sigma * v[i];
+        re[i] = std::cos(x);
+        im[i] = std::sin(x);
+    }
+    const std::vector<double> a = antialias(g);
+    const Plan2 plan = make_plan2(nx, ny);
+    Work2 ws;
+    fft2(plan, re, im, -1, ws, nullptr, nullptr, a.data(), nullptr);
+    fft2(plan, re, im, +1, ws, nullptr, nullptr, nullptr, nullptr, 1.0 / (double)N);
+    return 0;
+}
+
+// The Fresnel propagator of a slice dz [A] (Multislice.swift:108-130): e^{-i pi lambda dz k^2} A, times the tilt phase
+// e^{-2 pi i dz (kx tan tx + ky tan ty)} for a beam tilt (tx, ty) [mrad].
+int simk_cpu_propagator(int nx, int ny, double ex, double ey, double energy, double dz, double tilt_x, double tilt_y,
+                        double* re, double* im) {
+    if (nx < 1 || ny < 1 || !(ex > 0 && ey > 0 && energy > 0)) return 1;
+    const Geo g{nx, ny, ex, ey};
+    const double lam = wavelength(energy);
+    const std::vector<double> kx = fftfreq(nx, g.dx()), ky = fftfreq(ny, g.dy()), a = antialias(g);
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            const size_t i = (size_t)ix * ny + iy;
+            const double k2 = kx[ix] * kx[ix] + ky[iy] * ky[iy];
+            const double x = -k2 * M_PI * dz * lam;
+            double pr = std::cos(x) * a[i], pi = std::sin(x) * a[i];
+            if (tilt_x != 0 || tilt_y != 0) {
+                const double t = -2 * M_PI * dz * (kx[ix] * std::tan(tilt_x / 1e3) + ky[iy] * std::tan(tilt_y / 1e3));
+                const double c = std::cos(t), sn = std::sin(t);
+                const double r2 = pr * c - pi * sn;
+                pi = pr * sn + pi * c;
+                pr = r2;
+            }
+            re[i] = pr;
+            im[i] = pi;
+        }
+    return 0;
+}
+
+// The probe's centred spectrum (Probe.swift:25-48, 113-136): the aperture (abTEM's soft edge one pixel wide when
+// `soft`; semiangle [mrad], INFINITY for none) times e^{-i chi} (25 aberrations in simk_probe's order), divided by its
+// norm.
+int simk_cpu_probe_spectrum(int nx, int ny, double ex, double ey, double energy, double semiangle, int soft,
+                            const double* aberrations, double* re, double* im) {
+    if (nx < 1 || ny < 1 || !(ex > 0 && ey > 0 && energy > 0)) return 1;
+    const Geo g{nx, ny, ex, ey};
+    const double lam = wavelength(energy);
+    const std::vector<double> kx = fftfreq(nx, g.dx()), ky = fftfreq(ny, g.dy());
+    const double rsx = 1.0 / (nx * g.dx()), rsy = 1.0 / (ny * g.dy());
+    const double cutoff = semiangle * 1e-3, dax = rsx * 1e3 * lam * 1e-3, day = rsy * 1e3 * lam * 1e-3;
+    double norm2 = 0.0;
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            const size_t i = (size_t)ix * ny + iy;
+            const double alpha = std::sqrt(kx[ix] * kx[ix] + ky[iy] * ky[iy]) * lam;
+            const double phi = std::atan2(ky[iy], kx[ix]);
+            double ap = 1.0;
+            if (!std::isinf(semiangle)) {
+                if (!soft) {
+                    ap = alpha <= cutoff ? 1.0 : 0.0;
+                } else if (ix == 0 && iy == 0) {
+                    ap = 1.0;
+                } else {
+                    const double a = std::cos(phi) * dax, b = std::sin(phi) * day;
+                    const double d = std::sqrt(a * a + b * b);
+                    ap = std::min(std::max((cutoff - alpha) / d + 0.5, 0.0), 1.0);
+                }
+            }
+            const double c = chi(alpha, phi, aberrations, lam);
+            re[i] = ap * std::cos(-c);
+            im[i] = ap * std::sin(-c);
+            norm2 += re[i] * re[i] + im[i] * im[i];
+        }
+    const double n = std::sqrt(norm2);
+    for (size_t i = 0; i < g.count(); ++i) {
+        re[i] /= n;
+        im[i] /= n;
+    }
+    return 0;
+}
+
+// An annular detector's mask on the k-space pixels (Detectors.swift:39-44, 119-135): inner^2 <= alpha^2 < outer^2,
+// alpha from fftfreq(m, 1 / d / m) with d the angular sampling [mrad / pixel]; out 1 or 0.
+int simk_cpu_annular_mask(int nx, int ny, double ex, double ey, double energy, double inner, double outer,
+                          double* out) {
+    if (nx < 1 || ny < 1 || !(ex > 0 && ey > 0 && energy > 0)) return 1;
+    const Geo g{nx, ny, ex, ey};
+    const double lam = wavelength(energy);
+    const double ax = 1.0 / (nx * g.dx()) * lam * 1e3, ay = 1.0 / (ny * g.dy()) * lam * 1e3;
+    const std::vector<double> fx = fftfreq(nx, 1.0 / ax / nx), fy = fftfreq(ny, 1.0 / ay / ny);
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            const double a2 = fx[ix] * fx[ix] + fy[iy] * fy[iy];
+            out[(size_t)ix * ny + iy] = (a2 >= inner * inner && a2 < outer * outer) ? 1.0 : 0.0;
+        }
+    return 0;
+}
+
+// GaussianGenerator (FrozenPhonons.swift:14-58): SplitMix64 seeding, xoshiro256**, Box-Muller using both outputs.
+int simk_cpu_normals(uint64_t seed, int n, double* out) {
+    if (n < 0) return 1;
+    auto fin = [](uint64_t z) {
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    };
+    uint64_t st[4], x = seed;
+    for (int i = 0; i < 4; ++i) {
+        x += 0x9E3779B97F4A7C15ULL;
+        st[i] = fin(x);
+    }
+    auto rotl = [](uint64_t v, int k) { return (v << k) | (v >> (64 - k)); };
+    auto next = [&]() {
+        const uint64_t result = rotl(st[1] * 5, 7) * 9;
+        const uint64_t t = st[1] << 17;
+        st[2] ^= st[0];
+        st[3] ^= st[1];
+        st[1] ^= st[2];
+        st[0] ^= st[3];
+        st[2] ^= t;
+        st[3] = rotl(st[3], 45);
+        return result;
+    };
+    for (int i = 0; i < n; i += 2) {
+        const double u1 = (double)((next() >> 11) + 1) * 0x1p-53;
+        const double u2 = (double)(next() >> 11) * 0x1p-53;
+        const double r = std::sqrt(-2 * std::log(u1)), th = 2 * M_PI * u2;
+        out[i] = r * std::cos(th);
+        if (i + 1 < n) out[i + 1] = r * std::sin(th);
+    }
     return 0;
 }
 

@@ -3,8 +3,11 @@
 threads as runCPUParallel: Sources/SimulatoCore/Multislice.swift:132-157, Sources/SimulatoProbe/Probe.swift:113-156,
 Sources/SimulatoDetector/Detectors.swift:28-36, 119-135, Sources/SimulatoCore/MetalMultislice.swift:28-47).
 
-Only the tests and the benchmark's CPU legs use it, as a checker and as the timed CPU baseline; the CUDA library never
-does. The library is built by `make -C oracle/cpu` (or `build()` below) into oracle/_build/libsimk_cpu.so."""
+Besides the per-position loop it restates the per-potential set-up (Sources/SimulatoMultislice/ProjectedPotential.swift:
+110-201, Multislice.swift:83-130, Sources/SimulatoProbe/Probe.swift:25-48, 113-136, Detectors.swift:39-44, 119-135,
+FrozenPhonons.swift:14-58), so `ScanInputs.from_structure` builds a scan from atoms without the NumPy oracle; only the
+Lobato table comes from the oracle's data file. Only the tests and the benchmark's CPU legs use it, as a checker and as
+the timed CPU baseline; the CUDA library never does. The library is built by `make -C oracle/cpu` (or `build()` below) into oracle/_build/libsimk_cpu.so."""
 
 import ctypes as C
 import os
@@ -47,6 +50,19 @@ def lib():
         L.simk_cpu_factorization.restype = C.c_int
         L.simk_cpu_cost_guess.argtypes = [C.c_int]
         L.simk_cpu_cost_guess.restype = C.c_double
+        L.simk_cpu_potential.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _D, C.c_int,
+                                         _I, _D, C.c_int, _I, _D, _D, C.c_int, _D]
+        L.simk_cpu_transmission.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D, _D, _D]
+        L.simk_cpu_propagator.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, _D, _D]
+        L.simk_cpu_probe_spectrum.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.c_int, _D, _D, _D]
+        L.simk_cpu_annular_mask.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                            C.c_double, _D]
+        L.simk_cpu_normals.argtypes = [C.c_uint64, C.c_int, _D]
+        for f in ("simk_cpu_potential", "simk_cpu_transmission", "simk_cpu_propagator", "simk_cpu_probe_spectrum",
+                  "simk_cpu_annular_mask", "simk_cpu_normals"):
+            getattr(L, f).restype = C.c_int
         _lib = L
     return _lib
 
@@ -90,6 +106,66 @@ def fft2(a: np.ndarray, inverse: bool = False) -> np.ndarray:
     return (re + 1j * im).reshape(shape)
 
 
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise ValueError(f"{what}: bad arguments (status {rc})")
+
+
+def potential(s: "O.Structure", nx: int, ny: int, thicknesses, pi_choice: str = "exact") -> np.ndarray:
+    """The projected potential of every slice [S][nx][ny] by the C++ restatement (wrap, slicing, bilinear deltas,
+    f(k^2) / S(k) per element), with the Lobato table the oracle reads."""
+    numbers = np.ascontiguousarray(s.numbers, dtype=np.int32)
+    elements = sorted(set(int(z) for z in numbers))
+    tz = np.array(elements, dtype=np.int32)
+    ta = np.ascontiguousarray([O.lobato_parameters(z)[0] for z in elements], dtype=np.float64).reshape(-1)
+    tb = np.ascontiguousarray([O.lobato_parameters(z)[1] for z in elements], dtype=np.float64).reshape(-1)
+    t = np.ascontiguousarray(thicknesses, dtype=np.float64)
+    xyz = np.ascontiguousarray(s.positions, dtype=np.float64).reshape(-1)
+    out = np.zeros((len(t), nx, ny))
+    _check(lib().simk_cpu_potential(nx, ny, s.box[0], s.box[1], s.box[2], len(t), _p(t), len(numbers),
+                                    numbers.ctypes.data_as(_I), _p(xyz), len(tz), tz.ctypes.data_as(_I),
+                                    _p(ta if ta.size else np.zeros(1)), _p(tb if tb.size else np.zeros(1)),
+                                    1 if pi_choice == "abtem" else 0, _p(out)), "simk_cpu_potential")
+    return out
+
+
+def transmission(v: np.ndarray, energy: float, g: "O.Grid") -> np.ndarray:
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    re, im = np.zeros_like(v), np.zeros_like(v)
+    _check(lib().simk_cpu_transmission(g.nx, g.ny, g.extent_x, g.extent_y, energy, _p(v), _p(re), _p(im)),
+           "simk_cpu_transmission")
+    return re + 1j * im
+
+
+def propagator(g: "O.Grid", energy: float, dz: float, tilt=(0.0, 0.0)) -> np.ndarray:
+    re, im = np.zeros((g.nx, g.ny)), np.zeros((g.nx, g.ny))
+    _check(lib().simk_cpu_propagator(g.nx, g.ny, g.extent_x, g.extent_y, energy, dz, float(tilt[0]), float(tilt[1]),
+                                     _p(re), _p(im)), "simk_cpu_propagator")
+    return re + 1j * im
+
+
+def probe_spectrum(p: "O.ProbeSpec", g: "O.Grid") -> np.ndarray:
+    ab = np.ascontiguousarray([float(p.aberrations.get(k, 0.0)) for k in O.ABERRATION_SYMBOLS], dtype=np.float64)
+    re, im = np.zeros((g.nx, g.ny)), np.zeros((g.nx, g.ny))
+    _check(lib().simk_cpu_probe_spectrum(g.nx, g.ny, g.extent_x, g.extent_y, p.energy, p.semiangle,
+                                         1 if p.soft else 0, _p(ab), _p(re), _p(im)), "simk_cpu_probe_spectrum")
+    return re + 1j * im
+
+
+def annular_mask(g: "O.Grid", energy: float, inner: float, outer: float) -> np.ndarray:
+    out = np.zeros((g.nx, g.ny))
+    _check(lib().simk_cpu_annular_mask(g.nx, g.ny, g.extent_x, g.extent_y, energy, inner, outer, _p(out)),
+           "simk_cpu_annular_mask")
+    return out
+
+
+def normals(seed: int, n: int) -> np.ndarray:
+    """The first n outputs of GaussianGenerator(seed)."""
+    out = np.zeros(n)
+    _check(lib().simk_cpu_normals(int(seed) & 0xFFFFFFFFFFFFFFFF, n, _p(out)), "simk_cpu_normals")
+    return out
+
+
 class ScanInputs:
     """The per-potential inputs of the scan, built once by the float64 NumPy oracle (they are shared by all positions,
     as runBatch shares them): transmissions, one propagator per distinct slice thickness, the probe's centred spectrum
@@ -114,6 +190,34 @@ class ScanInputs:
         self.fy = O.fftfreq(ny, 1.0).astype(np.float64)
         self.masks = np.ascontiguousarray(np.asarray(masks, dtype=np.float64).reshape(-1, nx, ny))
         self.n_slices = len(thicknesses)
+
+    @classmethod
+    def from_structure(cls, probe: "O.ProbeSpec", s: "O.Structure", nx: int, ny: int, thicknesses, detectors,
+                       pi_choice: str = "exact") -> "ScanInputs":
+        """Every input built by the C++ restatement: the potential, the transmissions, one propagator per distinct
+        thickness, the probe spectrum and the annular masks ((inner, outer) [mrad]; outer already checked against
+        the grid's largest angle)."""
+        g = O.Grid(nx, ny, s.box[0], s.box[1])
+        vs = potential(s, nx, ny, thicknesses, pi_choice)
+        self = cls.__new__(cls)
+        self.g = g
+        t = np.stack([transmission(v, probe.energy, g) for v in vs])
+        self.t_re, self.t_im = np.ascontiguousarray(t.real), np.ascontiguousarray(t.imag)
+        dzs = []
+        self.prop = np.zeros(len(thicknesses), dtype=np.int32)
+        for j, dz in enumerate(thicknesses):
+            if dz not in dzs:
+                dzs.append(dz)
+            self.prop[j] = dzs.index(dz)
+        pr = np.stack([propagator(g, probe.energy, dz, probe.tilt) for dz in dzs])
+        self.p_re, self.p_im = np.ascontiguousarray(pr.real), np.ascontiguousarray(pr.imag)
+        sp = probe_spectrum(probe, g)
+        self.s_re, self.s_im = np.ascontiguousarray(sp.real), np.ascontiguousarray(sp.imag)
+        self.fx = O.fftfreq(nx, 1.0).astype(np.float64)
+        self.fy = O.fftfreq(ny, 1.0).astype(np.float64)
+        self.masks = np.ascontiguousarray(np.stack([annular_mask(g, probe.energy, a, b) for a, b in detectors]))
+        self.n_slices = len(thicknesses)
+        return self
 
     def scan(self, positions, threads: int = 1) -> np.ndarray:
         """Detector values [position][detector] at `positions` (Angstrom)."""

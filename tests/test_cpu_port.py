@@ -3,6 +3,8 @@ the CPU baseline: its FFT path selection against the reference's pinned lengths 
 (Tests/SimulatoCoreTests/SimulatoCoreTests.swift:57-81), its transforms against NumPy's, and its scan against the NumPy
 oracle. CPU only."""
 
+import math
+
 import numpy as np
 import pytest
 
@@ -82,3 +84,51 @@ def test_scan_refuses_bad_arguments():
     assert si.scan(np.zeros((0, 2))).shape == (0, 1)
     with pytest.raises(ValueError):
         K.fft2(np.zeros((0, 4), dtype=complex))
+
+
+# ---- the per-potential set-up in C++ --------------------------------------------------------------------------------
+
+def test_setup_stages_match_numpy():
+    s = O.srtio3_cell().repeated(2, 2, 2)
+    for pi in ("exact", "abtem"):
+        op = O.Potential.from_structure(s, 64, 48, slice_thickness=1.9525, pi_choice=pi)
+        assert O.rel_max(K.potential(s, 64, 48, op.thicknesses, pi), np.array(op.build())) <= 1e-13
+    g = op.grid
+    v = op.build()[0]
+    assert O.rel_max(K.transmission(v, 200e3, g), O.transmission(v, 200e3, g)) <= 1e-13
+    for tilt in ((0.0, 0.0), (3.0, -2.0)):
+        assert O.rel_max(K.propagator(g, 200e3, 1.9525, tilt), O.propagator(g, 200e3, 1.9525, tilt)) <= 1e-13
+    for ab, soft, semi in [({}, True, 20.0), ({}, False, 20.0), ({}, True, math.inf),
+                           ({"C10": -50.0, "C30": 1e4, "C12": 20.0, "phi12": 0.3, "C23": 100.0, "phi23": 0.5,
+                             "C50": 1e6}, True, 25.0)]:
+        p = O.ProbeSpec(200e3, semi, ab, soft)
+        assert O.rel_max(K.probe_spectrum(p, g), O.centred_spectrum(p, g)) <= 1e-13
+    assert np.array_equal(K.annular_mask(g, 200e3, 30.0, 60.0), O.annular_mask(g, 200e3, 30.0, 60.0).astype(float))
+    gen = O.GaussianGenerator(7)
+    assert np.array_equal(K.normals(7, 9), np.array([gen.next_normal() for _ in range(9)]))
+
+
+@pytest.mark.parametrize("name", ["A1", "D1"])
+def test_cpp_potential_is_pinned_to_the_reference(name):
+    # the reference's abTEM fixtures at its own bound (PotentialPinsTests.swift: 1e-11 with abTEM's float32 pi)
+    import golden_io as G
+    c = G.case("slice-1", name)
+    s = O.Structure(tuple(c["box"]), np.array(c["numbers"], dtype=int),
+                    np.array(c["positions"], dtype=np.float64).reshape(-1, 3))
+    v = K.potential(s, c["gpts"][0], c["gpts"][1], c["slice_thickness"], "abtem")
+    for j in range(c["V_stored_slices"]):
+        assert O.rel_max(v[j], G.array("slice-1", f"{name}.V.{j}")) <= 1e-11
+
+
+def test_a_scan_built_in_cpp_matches_the_oracle():
+    s = O.srtio3_cell().repeated(2, 2, 2)
+    op = O.Potential.from_structure(s, 64, 48, slice_thickness=1.9525)
+    spec = O.ProbeSpec(200e3, 20.0, {"C10": -30.0})
+    dets = [(0.0, 20.0), (30.0, 60.0)]
+    pos = O.grid_scan_positions((0.0, 0.0), (3.905, 3.905), 3, 3)
+    ores = O.stem_scan(spec, [(op.grid, op.build(), op.thicknesses)], pos,
+                       [O.DetectorSpec("annular", {"inner": a, "outer": b}) for a, b in dets])
+    got = K.ScanInputs.from_structure(spec, s, 64, 48, op.thicknesses, dets).scan(pos, threads=2)
+    for d in range(len(dets)):
+        r = np.asarray(ores[d]).ravel()
+        assert np.abs(got[:, d] - r).max() <= 1e-12 * np.abs(r).max()
