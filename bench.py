@@ -200,6 +200,22 @@ def traffic_from_profiles(kernel: str):
 # CPU: the reference's path restated (oracle), on host threads over positions
 # ---------------------------------------------------------------------------------------------------------------------
 
+def slowest_rank(value: float, dist=None, device: str = "cpu") -> float:
+    """The largest of every rank's `value` (a time): the whole job's time when each rank runs the same work. Every rank
+    calls it at the same point; without a process group it returns `value`."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world: int, slowest_seconds: float) -> float:
+    """Units all ranks processed per second of the slowest rank (replicas: every rank does the same work)."""
+    return world * units_per_rank / slowest_seconds
+
+
 def sample_indices(n_positions: int):
     """The positions of the scan the CPU legs run: every (4096 / n)-th position."""
     return np.arange(SCAN_N * SCAN_N)[:: max(1, (SCAN_N * SCAN_N) // n_positions)][:n_positions]
@@ -782,12 +798,8 @@ def main():
     names = ["fused_rows", "fused_cols", "line_fft", "pointwise", "detect"]
     ktimes = {n: engine.kernel_time(n) for n in names}
     engine.set_timing(False)
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * steps_per_scan * args.steps / (ms_max / 1e3)
+    ms_max = slowest_rank(ms, dist, "cuda")
+    value = whole_job_rate(steps_per_scan * args.steps, world, ms_max / 1e3)
 
     # dominant kernel: the largest total time
     dom = max(ktimes, key=lambda n: ktimes[n][0])
@@ -820,7 +832,7 @@ def main():
             if it > 0:
                 times.append(time.perf_counter() - t0)
             del p2
-        e2e_val = world * steps_per_scan / statistics.median(times)
+        e2e_val = whole_job_rate(steps_per_scan, world, slowest_rank(statistics.median(times), dist, "cuda"))
         n_atoms = len(nums)
         h2d = n_atoms * (4 + 24 + 4) + 20 * 8 + n_pos * 16
         d2h = sum(n_pos * 8 for _ in dets)
