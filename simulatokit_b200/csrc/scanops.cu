@@ -10,7 +10,6 @@
 // GPU cannot split), so a seed gives the same noise on every run and any split of the work, not the reference's bits.
 #include <algorithm>
 #include <cmath>
-#include <set>
 
 #include "fft.cuh"
 #include "scanops.cuh"
@@ -393,12 +392,9 @@ void gaussian_source_size_device(Context& ctx, int nx, int ny, long long v, doub
         {
             KernelTimer t(ctx, "gauss_axis", 16.0 * (double)total);
             if (stride >= 32 && rows <= kMaxStagedRows) {
-                static std::set<int> opted_in;  // devices whose launch limit was raised (under the context lock)
-                if (!opted_in.count(ctx.device)) {
-                    SIMK_CUDA(cudaFuncSetAttribute(k_gauss_axis_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   2 * kStagedAlloc * 32 * (int)sizeof(double)));
-                    opted_in.insert(ctx.device);
-                }
+                // the launch limit for this device (set on every call: contexts on other threads may do the same)
+                SIMK_CUDA(cudaFuncSetAttribute(k_gauss_axis_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               2 * kStagedAlloc * 32 * (int)sizeof(double)));
                 const long long outer = total / ((long long)L * stride);
                 const int KT = staged_outputs(L, radius);
                 const long long col_tiles = (stride + 31) / 32;
