@@ -452,6 +452,7 @@ int simk_gaussian_source_size(simk_context* ctx, int32_t nx, int32_t ny, int64_t
     return guarded([&] {
         SIMK_REQUIRE(ctx && in && out, "null argument");
         SIMK_REQUIRE(nx >= 1 && ny >= 1 && value_count >= 1, "the scan needs at least one position and one value");
+        SIMK_REQUIRE(value_count <= (1LL << 40) / ((long long)nx * ny), "the scan holds more than 2^40 values");
         std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
         activate(ctx->impl);
         Context& c = ctx->impl;
@@ -481,6 +482,7 @@ int simk_poisson_noise(simk_context* ctx, int64_t count, const double* in, doubl
         SIMK_REQUIRE(ctx && (count == 0 || (in && out)), "null argument");
         SIMK_REQUIRE(count >= 0, "negative value count");
         SIMK_REQUIRE(samples >= 1, "samples must be at least 1, got " + std::to_string(samples));
+        SIMK_REQUIRE(count <= (1LL << 40) / samples, "more than 2^40 values and samples");
         std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
         activate(ctx->impl);
         Context& c = ctx->impl;
@@ -515,6 +517,7 @@ int simk_integrate_gradient(simk_context* ctx, int32_t nx, int32_t ny, double sa
         SIMK_REQUIRE(nx >= 2 && ny >= 2, "the gradient's images need at least 2 points per axis, got " +
                                              std::to_string(nx) + " x " + std::to_string(ny));
         SIMK_REQUIRE(stride >= 1, "the component stride must be at least 1");
+        SIMK_REQUIRE((long long)nx * ny <= (1LL << 28), "the gradient's images hold more than 2^28 pixels");
         std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
         activate(ctx->impl);
         Context& c = ctx->impl;

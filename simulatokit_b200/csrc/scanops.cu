@@ -344,6 +344,7 @@ void gaussian_source_size_device(Context& ctx, int nx, int ny, long long v, doub
                  "the scan sampling must be finite and positive, got (" + std::to_string(sampling_x) + ", " +
                      std::to_string(sampling_y) + ") A");
     SIMK_REQUIRE(nx >= 1 && ny >= 1 && v >= 1, "the scan needs at least one position and one value");
+    SIMK_REQUIRE(v <= (1LL << 40) / ((long long)nx * ny), "the scan holds more than 2^40 values");
     SIMK_REQUIRE((uintptr_t)in % sizeof(double) == 0 && (uintptr_t)out % sizeof(double) == 0,
                  "the values must be 8-byte aligned float64 arrays");
     const long long total = (long long)nx * ny * v;
@@ -426,6 +427,7 @@ void poisson_noise_device(Context& ctx, long long count, const double* in, doubl
     SIMK_REQUIRE(samples >= 1, "samples must be at least 1, got " + std::to_string(samples));
     SIMK_REQUIRE(count >= 0, "negative value count");
     SIMK_REQUIRE(samples == 1 || out != in, "several samples cannot overwrite their input");
+    SIMK_REQUIRE(count <= (1LL << 40) / samples, "more than 2^40 values and samples");
     if (count == 0) return;
     ctx.post_flag.ensure(sizeof(int));
     SIMK_CUDA(cudaMemsetAsync(ctx.post_flag.ptr, 0, sizeof(int), ctx.stream));
@@ -450,6 +452,7 @@ void integrate_gradient_device(Context& ctx, int nx, int ny, double sampling_x, 
     SIMK_REQUIRE(nx >= 2 && ny >= 2, "the gradient's images need at least 2 points per axis, got " +
                                          std::to_string(nx) + " x " + std::to_string(ny));
     SIMK_REQUIRE(stride >= 1, "the component stride must be at least 1");
+    SIMK_REQUIRE((long long)nx * ny <= (1LL << 28), "the gradient's images hold more than 2^28 pixels");
     const long long n = (long long)nx * ny;
     ctx.post_spectra.ensure(2 * n * sizeof(double2));
     ctx.post_min.ensure(sizeof(double));

@@ -200,3 +200,15 @@ def test_icom_of_the_devices_own_scan_stays_on_the_device(engine):
         # the device integration of the device's own centre of mass equals the host form's
         m = sk.ScanMeasurement([gx, gy], [2], o.cpu().numpy())
         assert O.rel_max(got, m.integratedCenterOfMass(sx, sy, engine=engine).values) <= 1e-14, tag
+
+
+def test_sizes_past_the_limits_are_refused_before_any_work(engine):
+    small = np.zeros(4)
+    st = engine.lib.simk_gaussian_source_size(engine.handle, 1 << 15, 1 << 15, 1 << 20, 1.0, 1.0, 1.0, 1.0,
+                                              L.dptr(small), L.dptr(small))
+    assert st == L.SIMK_ERR_INVALID
+    st = engine.lib.simk_poisson_noise(engine.handle, 1 << 40, L.dptr(small), 1.0, 2, 1, L.dptr(small))
+    assert st == L.SIMK_ERR_INVALID
+    st = engine.lib.simk_integrate_gradient(engine.handle, 1 << 15, 1 << 15, 1.0, 1.0, L.dptr(small), L.dptr(small),
+                                            1, L.dptr(small))
+    assert st == L.SIMK_ERR_INVALID
