@@ -6,7 +6,6 @@ positions; a pixelated detector on a 128 x 128 grid up to 60 mrad (binned, this 
 centre-of-mass detector. Bounds: <= 1e-4 relative L2 per detector image for every form.
 """
 
-import numpy as np
 import pytest
 
 from oracle import simk_oracle as O
