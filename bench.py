@@ -185,14 +185,17 @@ class ClockSampler:
 
 
 def traffic_from_profiles(kernel: str):
-    """dram bytes per launch of `kernel` on this workload from the committed ncu summary, or None."""
+    """(dram bytes per launch, where they come from) of `kernel` on this workload from the committed ncu capture, or
+    (None, None). The figure is not measured in this run: it is the one-pass ncu capture named in the file, and it
+    goes stale when the kernel changes after that capture."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
         v = d.get(kernel)
         if isinstance(v, dict):
-            return v.get("dram_bytes_per_launch")
-    return None
+            return v.get("dram_bytes_per_launch"), f"profiles/roofline_traffic.json ({d.get('_captured', 'undated')}, " \
+                                                   f"{v.get('kernel')}), not measured in this run"
+    return None, None
 
 
 # ---------------------------------------------------------------------------------------------------------------------
@@ -220,25 +223,44 @@ def sample_indices(n_positions: int):
     return np.arange(SCAN_N * SCAN_N)[:: max(1, (SCAN_N * SCAN_N) // n_positions)][:n_positions]
 
 
+class CpuReference:
+    """The C++ float64 restatement of STEM.cpuScan (oracle/cpu/simk_cpu.cpp: FFT2D's mixed-radix / Bluestein
+    transforms, runCPU, Probe.build, the annular detectors) on a sample of the workload's positions, `threads` workers
+    over positions as runCPUParallel. The potential, transmissions, propagators, probe spectrum and masks are built
+    once, by the same C++ restatement, when the object is made, as runBatch shares them."""
+
+    def __init__(self, n_positions: int, threads: int):
+        from oracle import simk_cpu as K
+        from oracle import simk_oracle as O
+        box, nums, pos = srtio3(8, 8, 20)
+        s = O.Structure(box, nums, pos)
+        self.n_slices = len(O.slice_thicknesses(box[2], SLICE))
+        self.inputs = K.ScanInputs.from_structure(O.ProbeSpec(ENERGY, SEMIANGLE), s, NX, NY,
+                                                  O.slice_thicknesses(box[2], SLICE),
+                                                  [(a, b) for _, a, b in DETECTORS])
+        self.positions = scan_positions()[sample_indices(n_positions)]
+        self.threads = threads
+
+    def warm_up(self):
+        """One scan of `threads` positions (each worker's FFT plans and buffers)."""
+        self.inputs.scan(self.positions[:self.threads], threads=self.threads)
+
+    def step(self):
+        """One timed scan of the sample: (steps/s, seconds, positions, values [position][detector])."""
+        t0 = time.perf_counter()
+        vals = self.inputs.scan(self.positions, threads=self.threads)
+        dt = time.perf_counter() - t0
+        return len(self.positions) * self.n_slices / dt, dt, len(self.positions), vals
+
+
 def cpu_reference(n_positions: int, threads: int, want_values: bool = False):
-    """Times the C++ float64 restatement of STEM.cpuScan (oracle/cpu/simk_cpu.cpp: FFT2D's mixed-radix / Bluestein
-    transforms, runCPU, Probe.build, the annular detectors) on `n_positions` positions of the workload, `threads`
-    workers over positions as runCPUParallel. The potential, transmissions, propagators, probe spectrum and masks are
-    built once beforehand by the same C++ restatement, as runBatch shares them. Returns (steps/s, seconds, positions)
-    and, with want_values, the detector values at those positions ([detector][position])."""
-    from oracle import simk_cpu as K
-    from oracle import simk_oracle as O
-    box, nums, pos = srtio3(8, 8, 20)
-    s = O.Structure(box, nums, pos)
-    spec = O.ProbeSpec(ENERGY, SEMIANGLE)
-    thicknesses = O.slice_thicknesses(box[2], SLICE)
-    inputs = K.ScanInputs.from_structure(spec, s, NX, NY, thicknesses, [(a, b) for _, a, b in DETECTORS])
-    positions = scan_positions()[sample_indices(n_positions)]
-    inputs.scan(positions[:1], threads=1)  # warm-up
-    t0 = time.perf_counter()
-    vals = inputs.scan(positions, threads=threads)
-    dt = time.perf_counter() - t0
-    out = (len(positions) * len(thicknesses) / dt, dt, len(positions))
+    """One warm-up and one timed scan of the C++ float64 restatement on `n_positions` positions of the workload.
+    Returns (steps/s, seconds, positions) and, with want_values, the detector values at those positions
+    ([detector][position])."""
+    ref = CpuReference(n_positions, threads)
+    ref.warm_up()
+    v, dt, n, vals = ref.step()
+    out = (v, dt, n)
     if want_values:
         return out + ([vals[:, d].copy() for d in range(len(DETECTORS))],)
     return out
@@ -253,12 +275,12 @@ def run_reference(args):
     if rank != 0:
         return
     threads = min(8, os.cpu_count() or 1)
-    n_pos = args.cpu_positions
+    ref = CpuReference(args.cpu_positions, threads)
+    for _ in range(args.warmup):
+        ref.warm_up()
     vals = []
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
     for _ in range(args.steps):
-        v, dt, n = cpu_reference(n_pos, threads)
+        v, dt, n, _ = ref.step()
         vals.append(v)
     value = statistics.median(vals)
     line = {"metric": "probe.slice steps/s", "value": value, "unit": "probe.slice steps/s", "n_gpus": args.gpus,
@@ -804,11 +826,12 @@ def main():
     dom = max(ktimes, key=lambda n: ktimes[n][0])
     dms, dn, dbytes = ktimes[dom]
     peak, peak_kind = measured_peaks()
+    traffic, traffic_source = traffic_from_profiles(f"{dom}@{args.form}")
     achieved = (dbytes / dn) / (dms / dn / 1e3) / 1e9 if dn else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6.65 TB/s",
-                "traffic": traffic_from_profiles(f"{dom}@{args.form}"),
+                "traffic": traffic, "traffic_source": traffic_source,
                 "algorithmic_bytes_per_launch": dbytes / dn if dn else None,
                 "avg_launch_ms": dms / dn if dn else None,
                 "kernel_share": {n: round(ktimes[n][0] / ms_k, 4) for n in names if ktimes[n][1]},
@@ -857,6 +880,10 @@ def main():
             form_values[f] = [o.cpu().numpy().copy() for o in outs]
         engine.apply(opts)
         engine.set_stream(stream.cuda_stream)
+        if "bf16x3" in forms and "fused" in forms and "plain" in forms:
+            forms["bf16x3_over_fused"] = forms["bf16x3"]["value"] / forms["fused"]["value"]
+            forms["bf16x3_over_plain"] = forms["bf16x3"]["value"] / forms["plain"]["value"]
+            forms["fused_over_plain"] = forms["fused"]["value"] / forms["plain"]["value"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -10,7 +10,7 @@
  * SimulatoKit's `ComplexField` (Sources/SimulatoCore/Fields.swift:8-49), so a Swift caller passes `field.real` and
  * `field.imaginary` directly. Inside, waves are interleaved complex64 [batch][ix][iy] in HBM.
  *
- * Each function names the reference interface it replaces. The Swift-side binding is shown in INTEGRATION.md.
+ * Each function names the reference interface it replaces.
  */
 #ifndef SIMULATO_CUDA_H
 #define SIMULATO_CUDA_H
@@ -330,12 +330,14 @@ int simk_job_table_run(simk_context* ctx, int32_t n_jobs, const simk_job* jobs, 
  * No counterpart in the reference: an addition for callers that cannot let the library allocate device memory
  * (a host framework that owns all device memory through its own allocator, such as PyTorch's caching allocator or an
  * XLA custom call, where a cudaMalloc inside the call would bypass its accounting and may synchronise the device).
- * Writes Probe.centredSpectrum (the same values as simk_probe_spectrum, rounded to complex64, interleaved re, im,
- * nx x ny) into the caller's device buffer `out_device`, on `stream` (a cudaStream_t; NULL = the default stream),
- * without synchronising. It allocates nothing: its scratch is a fixed 32 KiB float64 array in the library's device
- * image, so grids above 2048 x 2048 pixels (4,194,304) are refused with SIMK_ERR_INVALID. The first call on a device
- * (with that device current) looks up the array's address; make it before any stream capture. Every call shares the
- * array: calls that overlap on the GPU race and must be serialised by the caller. */
+ * Writes the same values as simk_probe_spectrum, rounded to complex64 (interleaved re, im, nx x ny), into the
+ * caller's device buffer `out_device`, on `stream` (a cudaStream_t; NULL = the default stream), without
+ * synchronising. It allocates nothing: its scratch is a fixed 32 KiB float64 array in the library's device image, so
+ * grids above 2048 x 2048 pixels (4,194,304) are refused with SIMK_ERR_INVALID. The first call on a device (with that
+ * device current) looks up the array's address; make it before any stream capture. Calls that are not captured look
+ * the address up again (it belongs to the current context). A CUDA error already pending on the calling thread is
+ * returned as SIMK_ERR_CUDA and left pending; nothing is launched then. Every call shares the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 int simk_probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void* out_device, void* stream);
 
 /* ---- the transform itself (FFT2D, Sources/SimulatoCore/FFT2D.swift:169-265) ----------------------------------------

@@ -15,7 +15,14 @@
 // host threads without ordering) race on the shared array and must be serialised by the caller.
 //
 // Set-up: the first call on a device, with that device current, looks up the array's device address with
-// cudaGetSymbolAddress and caches it; make that first call before any stream capture.
+// cudaGetSymbolAddress and caches it; make that first call before any stream capture. The address belongs to the
+// context the call runs in (the device's primary context, as the runtime API uses), so every later call that is not
+// being captured looks it up again, which allocates nothing: a cudaDeviceReset between calls then cannot leave a stale
+// pointer behind. A call made while its stream is being captured uses the cached address.
+//
+// Errors: a CUDA error already pending on the calling thread (left by the host framework's own work) is reported as
+// such and left pending for its owner; nothing is launched then. Otherwise a launch error of this call is reported and
+// cleared.
 #include <mutex>
 
 #include "common.cuh"
@@ -119,13 +126,18 @@ __global__ void k_noalloc_write(NoallocProbe p, long long N, const double* scrat
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoallocMaxDevices] = {};
 
-// The device address of the scratch array on the current device, looked up once per device.
-double* noalloc_scratch_address() {
+// The device address of the scratch array on the current device: looked up on the first call and on every call whose
+// stream is not being captured; a call under capture takes the address cached by an earlier call.
+double* noalloc_scratch_address(cudaStream_t stream) {
     int dev = 0;
     SIMK_CUDA(cudaGetDevice(&dev));
     SIMK_REQUIRE(dev >= 0 && dev < kNoallocMaxDevices, "device ordinal out of range");
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    SIMK_CUDA(cudaStreamIsCapturing(stream, &capture));
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || capture == cudaStreamCaptureStatusNone) {
+        SIMK_REQUIRE(capture == cudaStreamCaptureStatusNone,
+                     "simk_probe_spectrum_noalloc: the first call on a device must come before any stream capture");
         void* ptr = nullptr;
         SIMK_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
         g_noalloc_ptr[dev] = static_cast<double*>(ptr);
@@ -162,14 +174,19 @@ void probe_spectrum_noalloc(const simk_grid* grid, const simk_probe* probe, void
     p.dax = 1.0 / ((double)p.nx * p.dx) * 1e3 * p.lambda * 1e-3;
     p.day = 1.0 / ((double)p.ny * p.dy) * 1e3 * p.lambda * 1e-3;
     for (int i = 0; i < 25; ++i) p.ab[i] = probe->aberrations[i];
-    double* scratch = noalloc_scratch_address();
+    // an error someone else left pending stays theirs: report it without clearing it, and launch nothing
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+        throw Error(SIMK_ERR_CUDA, std::string("simk_probe_spectrum_noalloc: a CUDA error was already pending on this "
+                                               "thread (") + cudaGetErrorString(pending) + "); nothing was launched");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* scratch = noalloc_scratch_address(s);
     const int blocks = (int)((N + kNoallocChunk - 1) / kNoallocChunk);
     k_noalloc_partials<<<blocks, 256, 0, s>>>(p, N, scratch);
     k_noalloc_total<<<1, 256, 0, s>>>(scratch, blocks);
     const int wblocks = (int)std::min<long long>((N + 255) / 256, 148LL * 16);
     k_noalloc_write<<<wblocks, 256, 0, s>>>(p, N, scratch, static_cast<float2*>(out_device));
-    SIMK_CUDA(cudaGetLastError());
+    SIMK_CUDA(cudaGetLastError());  // none was pending before the launches: an error here is this call's
 }
 
 }  // namespace simk

@@ -8,8 +8,8 @@ Writes, from the one source:
   simulatokit_b200/data/lobato.json        (for the Python host code and the CPU oracle)
   simulatokit_b200/csrc/lobato_table.inc   (compiled into libsimulato_cuda.so)
 
-Usage: python simulatokit_b200/data/make_lobato_table.py [path/to/LobatoTable.swift]
-(default: the reference checkout at /root/reference).
+Usage: python simulatokit_b200/data/make_lobato_table.py path/to/Sources/SimulatoMultislice/LobatoTable.swift
+(the file of a SimulatoKit checkout; required).
 """
 
 from __future__ import annotations
@@ -20,7 +20,6 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SOURCE = "/root/reference/Sources/SimulatoMultislice/LobatoTable.swift"
 
 
 def parse(text: str) -> list[tuple[int, str, list[float], list[float]]]:
@@ -34,7 +33,9 @@ def parse(text: str) -> list[tuple[int, str, list[float], list[float]]]:
 
 
 def main() -> None:
-    src = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SOURCE
+    if len(sys.argv) != 2:
+        sys.exit("usage: python simulatokit_b200/data/make_lobato_table.py path/to/LobatoTable.swift")
+    src = sys.argv[1]
     rows = parse(open(src).read())
     assert [r[0] for r in rows] == list(range(1, 104)), "expected Z = 1..103 in order"
     assert all(len(r[2]) == 5 and len(r[3]) == 5 for r in rows)

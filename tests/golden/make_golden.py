@@ -6,7 +6,7 @@ little-endian, complex interleaved; sha256 recorded in each JSON and checked her
 the JSON scalars are kept whole (minus the array index). The GPU box has no reference checkout, so the tests read
 only what this script writes.
 
-Usage: python tests/golden/make_golden.py [/path/to/SimulatoKit]   (default /root/reference)
+Usage: python tests/golden/make_golden.py /path/to/SimulatoKit   (the checkout's root; required)
 """
 
 from __future__ import annotations
@@ -51,7 +51,9 @@ def load(root: str, name: str):
 
 
 def main() -> None:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/SimulatoKit")
+    root = sys.argv[1]
     all_meta = {}
     for name, keep in KEEP.items():
         meta, arrays = load(root, name)
