@@ -40,6 +40,30 @@ struct DetectorPlan {
         DeviceBuffer xp, xi, xw, yp, yi, yw;  // int32 ptr [nb + 1], int32 pixel, float64 weight
     };
     std::vector<std::unique_ptr<Binned>> binned;
+    // Pixelated or binned detectors are present: they read the k-space waves the last column pass stores.
+    bool has_pixel_outputs = false;
+    int grid_ny = 0;
+    std::vector<int> host_chan_pix;
+    std::vector<float> host_chan_w;
+    // The channel lists regrouped for detection inside the fused form's last column pass, for column tiles of `tc`
+    // columns: the entries of column group g (columns g tc .. g tc + tc - 1) and channel ch, in increasing local index
+    // ix tc + (iy - g tc), at ent[ptr[g C + ch] .. ptr[g C + ch + 1]) as (local index, float bits of the weight).
+    struct TileChannels {
+        int tc = 0, groups = 0;
+        DeviceBuffer ptr;  // int32 [groups C + 1]
+        DeviceBuffer ent;  // int2 [total]
+    };
+    std::vector<std::unique_ptr<TileChannels>> tile_channels;
+    // Built on first use per tile width (allocates and copies: not inside a stream capture).
+    const TileChannels& tiles(int tc);
+};
+
+// Detection inside the fused form's last column pass (MODE 3): the plan, the per-(wave, column group, channel)
+// float64 partial sums it writes, and whether the pass must also store the k-space waves (pixelated / binned).
+struct FusedDetect {
+    DetectorPlan* plan = nullptr;
+    double* partial = nullptr;
+    int store = 0;
 };
 
 struct Propagator {
@@ -143,6 +167,8 @@ struct Context {
     std::map<std::tuple<int, int, double, double, double, double, double, double>, std::unique_ptr<Propagator>> props;
     // workspaces
     DeviceBuffer work_a, work_b, work_c, rx, ry, positions, partial;
+    // float64 channel partial sums of the detection fused into the last column pass: [wave][column group][channel]
+    DeviceBuffer det_partial;
     // scan post-processing: the Gaussian passes' intermediate, their weights, the Poisson sampler's status word, the
     // gradient integration's two spectra and its minimum
     DeviceBuffer post_work, post_weights, post_flag, post_spectra, post_min;
@@ -155,6 +181,7 @@ struct Context {
     struct SliceGraph {
         cudaGraphExec_t exec = nullptr;
         int64_t launches = 0;
+        int det_groups = 0;  // column groups of the detection fused into the last pass (0: none)
     };
     std::map<std::string, SliceGraph> slice_graphs;
     std::set<std::string> slice_seen;
@@ -216,8 +243,15 @@ void launch_mul_broadcast(Context& ctx, float2* psi, const float2* factor, long 
 std::unique_ptr<DetectorPlan> build_detector_plan(Context& ctx, const GridGeom& g, double energy,
                                                   const simk_detector* dets, int n_dets);
 void detector_shape(const GridGeom& g, double energy, const simk_detector& d, int* ndim, int* shape);
+// Every detector of the plan on the k-space waves phi; with channels = false only the pixelated and binned ones (the
+// channel detectors were summed inside the last column pass).
 void launch_detect(Context& ctx, const DetectorPlan& plan, const GridGeom& g, const float2* phi, int count,
-                   long long first_position, double* const* outputs_dev, double weight, float intensity_scale);
+                   long long first_position, double* const* outputs_dev, double weight, float intensity_scale,
+                   bool channels = true);
+// The channel detectors from the fused pass's partial sums: per (wave, channel) the sum over the `groups` column
+// groups in order, times weight, added to the detector's output.
+void launch_detect_fold(Context& ctx, const DetectorPlan& plan, const double* partial, int groups, int count,
+                        long long first_position, double* const* outputs_dev, double weight);
 
 }  // namespace simk
 

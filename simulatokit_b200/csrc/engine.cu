@@ -156,7 +156,7 @@ void scan_device(Context& ctx, const simk_probe& probe, const std::vector<Potent
         if (ctx.detector_plans.size() > 64) ctx.detector_plans.clear();
         dit = ctx.detector_plans.emplace(dkey, build_detector_plan(ctx, g, probe.energy, dets, n_det)).first;
     }
-    const DetectorPlan* dplan = dit->second.get();
+    DetectorPlan* dplan = dit->second.get();
     std::string skey = gkey + key_bytes(&probe, sizeof(simk_probe));
     auto sit = ctx.spectra.find(skey);
     if (sit == ctx.spectra.end()) {

@@ -39,19 +39,24 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
 bool fused_supported(Context& ctx, const GridGeom& g);
 // Every slice on `count` waves in place. probe_rows_pending: the waves come from the probe's column IFFT and still
 // need the row IFFT (and 1/N). After slice j the waves are in row-spectrum form (finish_rows completes them);
-// kspace_last: the last slice ends in k-space (P Phi) for the detectors. on_slice(j, kspace) after each slice.
-void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
-                     bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last);
+// kspace_last: the last slice ends in k-space (P Phi) for the detectors. on_slice(j, kspace) after each slice. With
+// `det` (and kspace_last) the last column pass sums the channel detectors in its epilogue where a TMA pass runs it:
+// returns the column groups of det->partial then, else 0.
+int propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
+                    bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last,
+                    const FusedDetect* det = nullptr);
 void finish_rows(Context& ctx, const GridGeom& g, float2* psi, int count);
-// The probes of positions [first, first + b) through every slice, left as FFT2(exit wave) in ctx.work_a.
-void exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
-                        const double* positions_dev, long long first, int b);
+// The probes of positions [first, first + b) through every slice, left as FFT2(exit wave) in ctx.work_a (unless `det`
+// took the channel detectors in the last pass and no pixelated or binned detector wants the waves; the return value is
+// propagate_fused's).
+int exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                       const double* positions_dev, long long first, int b, const FusedDetect* det = nullptr);
 // STEM.scan with a WavesDetector: the exit wave at every position (host positions), resampled in Fourier space to
 // rows x columns points (0, 0: the simulation grid), into host float64 arrays [position][row][column].
 void scan_waves(Context& ctx, const simk_probe& probe, PotentialImpl& pot, int n_pos, const double* positions_xy,
                 int rows, int columns, double* out_re, double* out_im);
 void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
-                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
+                      const double* positions_dev, long long first, int b, DetectorPlan& dplan,
                       double* const* outputs_dev, double weight);
 
 }  // namespace simk

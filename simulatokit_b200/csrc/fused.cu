@@ -164,6 +164,8 @@ struct ColArgs {
     const float2* ry;
     const int* p_row;  // job tables: wave b uses the propagator P + p_row[b] N (null: every wave uses P)
     int p_blocks;      // job tables: propagators stacked at P (for the tensor map)
+    FusedDetect det;   // mode 3: detection in the epilogue
+    int* det_groups;   // mode 3: receives the column groups of the partial sums (the launch's ny / TC)
 };
 
 // The propagator of wave b.
@@ -364,6 +366,50 @@ __global__ void __launch_bounds__(TC * (N / 8)) fused_cols_ct(ColArgs a, const f
     for (int i = 0; i < 8; ++i) col[(size_t)(t + T * i) * ny] = v[i];
 }
 
+// ---- detection in the last column pass's epilogue ----------------------------------------------------------------------
+// MODE 3 of the column pass: FFT -> x P as MODE 1, then every channel detector (annular, centre of mass, segmented) is
+// summed from the finished tile while it is still in shared memory, so the k-space wave need not be written and read
+// back (it is stored only when pixelated or binned detectors want it). Per (wave, column group, channel) one float64
+// partial: each thread sums its strided share of the group's entries in order, the warp reduces with shuffles, the
+// warps' sums are added in warp order; k_detect_fold then adds the groups in order. Fixed order throughout, so scans
+// stay bit-deterministic.
+struct DetectArgs {
+    const int* ptr;    // [groups C + 1]
+    const int2* ent;   // (local index ix TC + c, weight bits)
+    double* partial;   // [wave][groups][C]
+    int n_ch;          // C
+    int groups;        // ny / TC
+    int store;         // also store the k-space tile
+};
+
+// `tile`: the finished tile of wave b, column group g, natural [row][TC] layout; `red`: NT / 32 * C doubles of free
+// shared memory. Ends with the partials written; the caller's barrier must follow before `red` or `tile` is reused.
+template <int NT>
+__device__ __forceinline__ void detect_tile(const float2* __restrict__ tile, const DetectArgs& d, int b, int g, int tid,
+                                            double* __restrict__ red) {
+    constexpr int NW = NT / 32;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int* ptr = d.ptr + (size_t)g * d.n_ch;
+    for (int ch = 0; ch < d.n_ch; ++ch) {
+        const int e1 = __ldg(ptr + ch + 1);
+        double sum = 0.0;
+        for (int e = __ldg(ptr + ch) + tid; e < e1; e += NT) {
+            const int2 q = __ldg(d.ent + e);
+            const float2 v = tile[q.x];
+            sum += (double)((v.x * v.x + v.y * v.y) * __int_as_float(q.y));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) red[ch * NW + warp] = sum;
+    }
+    __syncthreads();
+    for (int ch = tid; ch < d.n_ch; ch += NT) {
+        double t = 0.0;
+        for (int w = 0; w < NW; ++w) t += red[ch * NW + w];
+        d.partial[((size_t)b * d.groups + g) * d.n_ch + ch] = t;
+    }
+}
+
 // ---- the persistent TMA-pipelined passes (power-of-two lengths) --------------------------------------------------------
 // Each CTA walks its tiles blockIdx.x, blockIdx.x + gridDim.x, ...: thread 0 starts the asynchronous copies of the
 // next tile (the waves and the matching rows of t or P) into the other shared-memory stage before the CTA transforms
@@ -416,7 +462,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
                                                                const __grid_constant__ CUtensorMap pmap,
                                                                float2* __restrict__ psi, float pscale, int ny,
                                                                int count, const float2* __restrict__ tw, int* err,
-                                                               const int* __restrict__ p_row) {
+                                                               const int* __restrict__ p_row, const DetectArgs det) {
     extern __shared__ __align__(128) unsigned char smem_tma[];
     constexpr int T = N / 8;
     constexpr int BOXH = tma_box_rows(N);
@@ -502,7 +548,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 v[i] = out[L::at(c, (int)t + T * i)];
-                if constexpr (MODE == 1) v[i] = cmul(v[i], pbuf[L::nat(c, (int)t + T * i)]) * pscale;
+                if constexpr (MODE == 1 || MODE == 3) v[i] = cmul(v[i], pbuf[L::nat(c, (int)t + T * i)]) * pscale;
             }
             __syncthreads();  // every thread has read `out`: it takes the tile in its natural [row][TC] layout
 #pragma unroll
@@ -520,7 +566,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 v[i] = out[L::at(c, (int)t + T * i)];
-                if constexpr (MODE == 1) v[i] = cmul(v[i], pbuf[L::nat(c, (int)t + T * i)]) * pscale;
+                if constexpr (MODE == 1 || MODE == 3) v[i] = cmul(v[i], pbuf[L::nat(c, (int)t + T * i)]) * pscale;
             }
             __syncthreads();  // every thread has read `out`: it takes the tile in its natural [row][TC] layout
 #pragma unroll
@@ -529,11 +575,17 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         }
         fence_proxy_async_shared();
         __syncthreads();  // every thread is done with the stage before its next copy
-        if (tid == 0) {
+        if (tid == 0 && (MODE != 3 || det.store)) {
             const int iy0 = iy - c;
 #pragma unroll
             for (int k = 0; k < NBOX; ++k) tma_store_2d(&map, store_src + k * BOXH * TC, 2 * iy0, b * N + k * BOXH);
             bulk_commit();
+        }
+        if constexpr (MODE == 3) {
+            // the P tile has been read: its space holds the warps' sums (TILE float2 >= NT / 32 * C doubles, C <= 64)
+            detect_tile<TC * T>(store_src, det, b, (iy - c) / TC, tid, reinterpret_cast<double*>(buf + TILE));
+            fence_proxy_async_shared();  // the sums were written by this proxy; the next copy into the stage by TMA
+            __syncthreads();  // the partials' reads of the tile and of the sums precede the next copy into the stage
         }
     }
     if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
@@ -860,9 +912,20 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
                                                   (unsigned long long)std::max(1, a.p_blocks) * N, 2 * TC, BOXH);
     const long long ntiles = (long long)count * (a.ny / TC);
     if (ntiles >= (1LL << 31)) return false;
+    DetectArgs det{};
+    if constexpr (MODE == 3) {
+        const DetectorPlan::TileChannels& tch = a.det.plan->tiles(TC);
+        det.ptr = tch.ptr.as<int>();
+        det.ent = tch.ent.as<int2>();
+        det.partial = a.det.partial;
+        det.n_ch = a.det.plan->n_channels;
+        det.groups = tch.groups;
+        det.store = a.det.store;
+        if (a.det_groups) *a.det_groups = tch.groups;
+    }
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(TC, T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
-                                                  ctx.err_flag.as<int>(), a.p_row);
+                                                  ctx.err_flag.as<int>(), a.p_row, det);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
@@ -873,6 +936,7 @@ bool launch_cols_tma(Context& ctx, const RegPlan& p, const ColArgs& a, int count
     if (TC < 2 || a.ny % TC) return false;  // the TMA box's inner extent must be a multiple of 16 bytes
     if (a.mode == 0) return launch_cols_tma_m<N, TC, 0, ENG>(ctx, p, a, count);
     if (a.mode == 1) return launch_cols_tma_m<N, TC, 1, ENG>(ctx, p, a, count);
+    if (a.mode == 3) return launch_cols_tma_m<N, TC, 3, ENG>(ctx, p, a, count);
     return false;
 }
 
@@ -920,6 +984,7 @@ bool cols_ct_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int
             default: break;
         }
     }
+    if (a.mode == 3) return false;  // detection in the epilogue runs on the TMA passes only
     switch (tc) {
         case 1: launch_cols_ct<N, 1>(ctx, p, a, count); return true;
         case 2: launch_cols_ct<N, 2>(ctx, p, a, count); return true;
@@ -1061,7 +1126,9 @@ void launch_rows(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul
     }
 }
 
-void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a_in, int count) {
+// Mode 3 (detection in the epilogue) where a TMA pass takes it, else mode 1; returns the column groups of the
+// detection's partial sums (0: the caller detects from the stored k-space waves).
+int launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a_in, int count) {
     ColArgs a = a_in;
     if (a.mode != 2 && ctx.wave_p) {  // job tables: per-wave propagators stacked at a.P
         a.p_row = ctx.wave_p;
@@ -1069,13 +1136,23 @@ void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a_in, int count)
     }
     const double bytes = (a.mode == 2 ? 8.0 : 16.0) * (double)p.n * a.ny * count;
     KernelTimer timer(ctx, "fused_cols", bytes);
+    int groups = 0;
+    if (a.mode == 3) {
+        a.det_groups = &groups;
+        const bool done = ctx.form == SIMK_FORM_BF16X3 ? cols_tc(ctx, p, a, count)
+                                                       : (cols_ct(ctx, p, a, count) ||
+                                                          (ctx.tma && cols_cc(ctx, p, a, count)));
+        if (done) return groups;
+        a.mode = 1;
+        groups = 0;
+    }
     if (ctx.form == SIMK_FORM_BF16X3 && a.mode != 2) {  // the probe's inverse transform (mode 2) stays float32
         if (!cols_tc(ctx, p, a, count))
             throw Error(SIMK_ERR_INVALID, "the bf16x3 form has no column pass for length " + std::to_string(p.n));
-        return;
+        return 0;
     }
-    if (cols_ct(ctx, p, a, count)) return;
-    if (ctx.tma && a.mode != 2 && cols_cc(ctx, p, a, count)) return;
+    if (cols_ct(ctx, p, a, count)) return 0;
+    if (ctx.tma && a.mode != 2 && cols_cc(ctx, p, a, count)) return 0;
     switch (p.E) {
         case 8: launch_cols_e<8>(ctx, p, a, count); break;
         case 12: launch_cols_e<12>(ctx, p, a, count); break;
@@ -1084,6 +1161,7 @@ void launch_cols(Context& ctx, const RegPlan& p, const ColArgs& a_in, int count)
         case 24: launch_cols_e<24>(ctx, p, a, count); break;
         default: throw Error(SIMK_ERR_INVALID, "unsupported register plan");
     }
+    return 0;
 }
 
 }  // namespace
@@ -1125,9 +1203,9 @@ bool fused_supported(Context& ctx, const GridGeom& g) {
 }
 
 namespace {
-void propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi,
-                           int count, bool probe_rows_pending, const std::function<void(int, bool)>& on_slice,
-                           bool kspace_last);
+int propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi,
+                          int count, bool probe_rows_pending, const std::function<void(int, bool)>& on_slice,
+                          bool kspace_last, const FusedDetect* det);
 
 template <typename T> void key_append(std::string& k, const T& v) {
     k.append(reinterpret_cast<const char*>(&v), sizeof(T));
@@ -1139,12 +1217,13 @@ template <typename T> void key_append(std::string& k, const T& v) {
 // propagators, the error flag and the launch configurations), the second time it is captured and instantiated, and
 // from then on one graph launch replaces the 2 S kernel launches. The key holds every pointer and setting the
 // recorded launches read, so a replay never sees a freed or different buffer.
-void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
-                     bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last) {
-    if (!ctx.graphs || ctx.timing || on_slice) {
-        propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, on_slice, kspace_last);
-        return;
-    }
+int propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi, int count,
+                    bool probe_rows_pending, const std::function<void(int, bool)>& on_slice, bool kspace_last,
+                    const FusedDetect* det) {
+    if (!kspace_last) det = nullptr;
+    if (!ctx.graphs || ctx.timing || on_slice)
+        return propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, on_slice, kspace_last,
+                                     det);
     std::string key;
     key_append(key, psi);
     key_append(key, count);
@@ -1157,23 +1236,29 @@ void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx,
     key_append(key, ctx.col_tile);
     key_append(key, ctx.tma);
     key_append(key, ctx.stream);
+    const FusedDetect nodet{};
+    const FusedDetect& d = det ? *det : nodet;
+    key_append(key, d.plan);
+    key_append(key, d.partial);
+    key_append(key, d.store);
     for (int j = 0; j < pot.n_slices(); ++j) key_append(key, ctx.propagator(pot.g, energy, pot.dz[j], tx, ty).p.ptr);
     auto it = ctx.slice_graphs.find(key);
     if (it != ctx.slice_graphs.end()) {
         SIMK_CUDA(cudaGraphLaunch(it->second.exec, ctx.stream));
         ctx.launches += it->second.launches;
-        return;
+        return it->second.det_groups;
     }
-    if (ctx.slice_seen.insert(key).second) {
-        propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, nullptr, kspace_last);
-        return;
-    }
+    if (ctx.slice_seen.insert(key).second)
+        return propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, nullptr, kspace_last,
+                                     det);
     if (ctx.slice_graphs.size() >= 64) ctx.drop_graphs();
     const int64_t before = ctx.launches;
     cudaGraph_t graph = nullptr;
+    int groups = 0;
     SIMK_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
     try {
-        propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, nullptr, kspace_last);
+        groups = propagate_fused_eager(ctx, pot, energy, tx, ty, psi, count, probe_rows_pending, nullptr, kspace_last,
+                                       det);
     } catch (...) {
         cudaStreamEndCapture(ctx.stream, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -1187,15 +1272,17 @@ void propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx,
     const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     SIMK_CUDA(e);
-    ctx.slice_graphs[key] = Context::SliceGraph{exec, n};
+    ctx.slice_graphs[key] = Context::SliceGraph{exec, n, groups};
     SIMK_CUDA(cudaGraphLaunch(exec, ctx.stream));
     ctx.launches += n;
+    return groups;
 }
 
 namespace {
-void propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi,
-                           int count, bool probe_rows_pending, const std::function<void(int, bool)>& on_slice,
-                           bool kspace_last) {
+int propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, double tx, double ty, float2* psi,
+                          int count, bool probe_rows_pending, const std::function<void(int, bool)>& on_slice,
+                          bool kspace_last, const FusedDetect* det) {
+    int groups = 0;
     const GridGeom& g = pot.g;
     const long long N = g.count();
     const RegPlan prow = reg_plan(ctx, g.ny);
@@ -1215,15 +1302,18 @@ void propagate_fused_eager(Context& ctx, PotentialImpl& pot, double energy, doub
         a.P = P.p.as<float2>();
         a.ny = g.ny;
         if (last && kspace_last) {
-            a.mode = 1;
+            a.mode = det ? 3 : 1;
+            if (det) a.det = *det;
             a.pscale = 1.0f;
         } else {
             a.mode = 0;
             a.pscale = invN;
         }
-        launch_cols(ctx, pcol, a, count);
+        const int gr = launch_cols(ctx, pcol, a, count);
+        if (last) groups = gr;
         if (on_slice) on_slice(j, last && kspace_last);
     }
+    return groups;
 }
 
 }  // namespace
@@ -1235,8 +1325,8 @@ void finish_rows(Context& ctx, const GridGeom& g, float2* psi, int count) {
     launch_rows(ctx, prow, psi, nullptr, g.nx, (long long)count * g.nx, 1, 0, 1.0f);
 }
 
-void exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
-                        const double* positions_dev, long long first, int b) {
+int exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
+                       const double* positions_dev, long long first, int b, const FusedDetect* det) {
     const GridGeom& g = pot.g;
     float2* psi = ctx.work_a.as<float2>();
     launch_ramps(ctx, g, positions_dev, first, b, ctx.rx.as<float2>(), ctx.ry.as<float2>());
@@ -1250,18 +1340,29 @@ void exit_spectra_fused(Context& ctx, PotentialImpl& pot, const simk_probe& prob
     a.ry = ctx.ry.as<float2>();
     a.pscale = 1.0f;
     launch_cols(ctx, pcol, a, b);
-    propagate_fused(ctx, pot, probe.energy, probe.tilt_x, probe.tilt_y, psi, b, true, nullptr, true);
+    return propagate_fused(ctx, pot, probe.energy, probe.tilt_x, probe.tilt_y, psi, b, true, nullptr, true, det);
 }
 
 void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe, const float2* spectrum,
-                      const double* positions_dev, long long first, int b, const DetectorPlan& dplan,
+                      const double* positions_dev, long long first, int b, DetectorPlan& dplan,
                       double* const* outputs_dev, double weight) {
     const GridGeom& g = pot.g;
     const long long N = g.count();
-    exit_spectra_fused(ctx, pot, probe, spectrum, positions_dev, first, b);
+    // channel detectors are summed in the last column pass when it runs on the TMA passes (at most 64 channels)
+    FusedDetect fd{};
+    const bool fuse = dplan.n_channels > 0 && dplan.n_channels <= 64 && ctx.tma;
+    if (fuse) {
+        ctx.det_partial.ensure((size_t)b * (g.ny / 2) * dplan.n_channels * sizeof(double));
+        fd.plan = &dplan;
+        fd.partial = ctx.det_partial.as<double>();
+        fd.store = dplan.has_pixel_outputs ? 1 : 0;
+    }
+    const int groups = exit_spectra_fused(ctx, pot, probe, spectrum, positions_dev, first, b, fuse ? &fd : nullptr);
     {
-        KernelTimer t(ctx, "detect", 8.0 * (double)N * b);
-        launch_detect(ctx, dplan, g, ctx.work_a.as<float2>(), b, first, outputs_dev, weight, 1.0f);
+        KernelTimer t(ctx, "detect", groups ? 0.0 : 8.0 * (double)N * b);
+        if (groups) launch_detect_fold(ctx, dplan, fd.partial, groups, b, first, outputs_dev, weight);
+        if (!groups || dplan.has_pixel_outputs)
+            launch_detect(ctx, dplan, g, ctx.work_a.as<float2>(), b, first, outputs_dev, weight, 1.0f, groups == 0);
     }
 }
 

@@ -3,6 +3,7 @@
 // the detector maps with their reduction kernel.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <numeric>
 
 #include "context.cuh"
@@ -809,6 +810,10 @@ std::unique_ptr<DetectorPlan> build_detector_plan(Context& ctx, const GridGeom& 
         ptr.push_back((int)pix.size());
     }
     plan->host_chan_ptr = ptr;
+    plan->host_chan_pix = pix;
+    plan->host_chan_w = w;
+    plan->grid_ny = g.ny;
+    plan->has_pixel_outputs = !crop.empty() || !plan->binned.empty();
     plan->total_entries = (long long)pix.size();
     plan->total_crop = (long long)crop.size();
     plan->chan_ptr.alloc(ptr.size() * sizeof(int));
@@ -826,6 +831,43 @@ std::unique_ptr<DetectorPlan> build_detector_plan(Context& ctx, const GridGeom& 
     return plan;
 }
 
+const DetectorPlan::TileChannels& DetectorPlan::tiles(int tc) {
+    for (auto& t : tile_channels)
+        if (t->tc == tc) return *t;
+    SIMK_REQUIRE(tc >= 1 && grid_ny % tc == 0, "column tile width must divide the grid");
+    auto t = std::make_unique<TileChannels>();
+    t->tc = tc;
+    t->groups = grid_ny / tc;
+    const int C = n_channels, G = t->groups;
+    std::vector<std::vector<std::pair<int, float>>> lists((size_t)G * C);
+    for (int ch = 0; ch < C; ++ch)
+        for (int e = host_chan_ptr[ch]; e < host_chan_ptr[ch + 1]; ++e) {
+            const int p = host_chan_pix[e], ix = p / grid_ny, iy = p % grid_ny;
+            lists[(size_t)(iy / tc) * C + ch].push_back({ix * tc + iy % tc, host_chan_w[e]});
+        }
+    std::vector<int> ptr(1, 0);
+    std::vector<int2> ent;
+    ent.reserve(host_chan_pix.size());
+    for (auto& l : lists) {
+        std::sort(l.begin(), l.end(), [](const std::pair<int, float>& a, const std::pair<int, float>& b) {
+            return a.first < b.first;
+        });
+        for (auto& e : l) {
+            int bits;
+            std::memcpy(&bits, &e.second, sizeof(int));
+            ent.push_back(make_int2(e.first, bits));
+        }
+        ptr.push_back((int)ent.size());
+    }
+    t->ptr.alloc(ptr.size() * sizeof(int));
+    SIMK_CUDA(cudaMemcpy(t->ptr.ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    t->ent.alloc(std::max<size_t>(1, ent.size()) * sizeof(int2));
+    if (!ent.empty())
+        SIMK_CUDA(cudaMemcpy(t->ent.ptr, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    tile_channels.push_back(std::move(t));
+    return *tile_channels.back();
+}
+
 // One block per (position, channel): sum over the channel's pixels of |phi|^2 * scale * w in float64, in a fixed
 // order (deterministic); adds weight * sum to the output of the channel's detector.
 struct ChannelOut {
@@ -834,6 +876,27 @@ struct ChannelOut {
     int count[16];
     int n_det;
 };
+
+__device__ __forceinline__ int channel_owner(const ChannelOut& co, int c) {
+    int d = 0;
+    for (int k = 0; k < co.n_det; ++k)
+        if (co.first_channel[k] >= 0 && c >= co.first_channel[k] && c < co.first_channel[k] + co.count[k]) d = k;
+    return d;
+}
+
+// One thread per (position, channel): the column groups' partial sums in order (the fused pass's fixed-order block
+// sums), weight times the total added to the channel's output.
+__global__ void k_detect_fold(const double* __restrict__ partial, int groups, int n_channels, int count,
+                              ChannelOut co, long long first_position, double weight) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count * n_channels) return;
+    const int b = i / n_channels, c = i - b * n_channels;
+    const double* p = partial + (size_t)b * groups * n_channels + c;
+    double s = 0.0;
+    for (int g = 0; g < groups; ++g) s += p[(size_t)g * n_channels];
+    const int d = channel_owner(co, c);
+    co.out[d][(first_position + b) * co.count[d] + (c - co.first_channel[d])] += weight * s;
+}
 
 __global__ void k_detect_channels(const float2* __restrict__ phi, long long N, const int* __restrict__ ptr,
                                   const int* __restrict__ pix, const float* __restrict__ w, int n_channels,
@@ -854,10 +917,7 @@ __global__ void k_detect_channels(const float2* __restrict__ phi, long long N, c
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        // which detector owns channel c
-        int d = 0;
-        for (int k = 0; k < co.n_det; ++k)
-            if (co.first_channel[k] >= 0 && c >= co.first_channel[k] && c < co.first_channel[k] + co.count[k]) d = k;
+        const int d = channel_owner(co, c);  // which detector owns channel c
         const int local = c - co.first_channel[d];
         double* o = co.out[d] + (first_position + b) * co.count[d] + local;
         *o += weight * part[0];
@@ -901,19 +961,40 @@ __global__ void k_detect_binned(const float2* __restrict__ phi, long long N, int
     }
 }
 
+namespace {
+ChannelOut channel_out(const DetectorPlan& plan, double* const* outputs_dev) {
+    const int nd = (int)plan.det_count.size();
+    SIMK_REQUIRE(nd <= 16, "at most 16 detectors per scan");
+    ChannelOut co{};
+    co.n_det = nd;
+    for (int d = 0; d < nd; ++d) {
+        co.out[d] = outputs_dev[d];
+        co.first_channel[d] = plan.det_first_channel[d];
+        co.count[d] = plan.det_count[d];
+    }
+    return co;
+}
+}  // namespace
+
+void launch_detect_fold(Context& ctx, const DetectorPlan& plan, const double* partial, int groups, int count,
+                        long long first_position, double* const* outputs_dev, double weight) {
+    if (plan.n_channels == 0 || count == 0) return;
+    const ChannelOut co = channel_out(plan, outputs_dev);
+    const int n = count * plan.n_channels;
+    k_detect_fold<<<(n + 127) / 128, 128, 0, ctx.stream>>>(partial, groups, plan.n_channels, count, co,
+                                                           first_position, weight);
+    ++ctx.launches;
+    SIMK_CUDA(cudaGetLastError());
+}
+
 void launch_detect(Context& ctx, const DetectorPlan& plan, const GridGeom& g, const float2* phi, int count,
-                   long long first_position, double* const* outputs_dev, double weight, float intensity_scale) {
+                   long long first_position, double* const* outputs_dev, double weight, float intensity_scale,
+                   bool channels) {
     const long long N = g.count();
     const int nd = (int)plan.det_count.size();
     SIMK_REQUIRE(nd <= 16, "at most 16 detectors per scan");
-    if (plan.n_channels > 0) {
-        ChannelOut co{};
-        co.n_det = nd;
-        for (int d = 0; d < nd; ++d) {
-            co.out[d] = outputs_dev[d];
-            co.first_channel[d] = plan.det_first_channel[d];
-            co.count[d] = plan.det_count[d];
-        }
+    if (channels && plan.n_channels > 0) {
+        const ChannelOut co = channel_out(plan, outputs_dev);
         dim3 grid(plan.n_channels, count);
         k_detect_channels<<<grid, 256, 0, ctx.stream>>>(phi, N, plan.chan_ptr.as<int>(), plan.chan_pix.as<int>(),
                                                         plan.chan_w.as<float>(), plan.n_channels, co, first_position,
