@@ -53,6 +53,14 @@ extern "C" {
 #define SIMK_OPT_TUNED_COL_TILE 9 /* read-only: the last tuning's choice (-1 before any) */
 #define SIMK_OPT_TUNED_TMA 10
 #define SIMK_OPT_TUNED_BATCH 11
+/* The bf16x3 form's radix-16 DFT stages on the fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
+ * memory) for grid sides 256 and 512, with the data split in three BF16 terms; 0 = the warp-level mma.sync stages
+ * (data in two terms) everywhere. Default 1. */
+#define SIMK_OPT_TCGEN05 12
+/* Sum the annular, centre-of-mass and segmented detectors inside the fused form's last column pass (TMA passes), so
+ * the k-space waves are neither written nor read back unless a pixelated or binned detector wants them; 0 = detect
+ * from the stored waves with separate kernels. Default 1. */
+#define SIMK_OPT_EPILOGUE_DETECT 13
 
 /* ---- Lobato pi choice (LobatoParameterization.PiConstant, LobatoParameterization.swift:15-24) ---- */
 #define SIMK_PI_EXACT 0

@@ -153,6 +153,8 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                 break;
             case SIMK_OPT_TMA: c.tma = value ? 1 : 0; break;
             case SIMK_OPT_AUTOTUNE: c.autotune = value ? 1 : 0; break;
+            case SIMK_OPT_TCGEN05: c.tcgen05 = value ? 1 : 0; break;
+            case SIMK_OPT_EPILOGUE_DETECT: c.epilogue_detect = value ? 1 : 0; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -194,6 +196,8 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_TMA: *value = c.tma; break;
             case SIMK_OPT_GRAPHS_CACHED: *value = (int64_t)c.slice_graphs.size(); break;
             case SIMK_OPT_AUTOTUNE: *value = c.autotune; break;
+            case SIMK_OPT_TCGEN05: *value = c.tcgen05; break;
+            case SIMK_OPT_EPILOGUE_DETECT: *value = c.epilogue_detect; break;
             case SIMK_OPT_TUNED_COL_TILE: *value = c.last_tuned.col_tile; break;
             case SIMK_OPT_TUNED_TMA: *value = c.last_tuned.tma; break;
             case SIMK_OPT_TUNED_BATCH: *value = c.last_tuned.batch; break;

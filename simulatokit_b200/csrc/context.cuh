@@ -148,6 +148,8 @@ struct Context {
     int graphs = 1;
     int col_tile = 0;
     int tma = 1;            // TMA-pipelined persistent column pass where available
+    int tcgen05 = 1;        // the bf16x3 form's DFT stages on tcgen05 where its tiles fit (else mma.sync)
+    int epilogue_detect = 1;  // channel detectors summed in the last column pass (TMA passes)
     int autotune = 0;       // time the launch configurations on first use of a (grid, form)
     struct Tuned {
         int col_tile = -1, tma = -1;

@@ -16,6 +16,7 @@
 
 #include "engine.cuh"
 #include "ccfft.cuh"
+#include "tc5fft.cuh"
 #include "tcfft.cuh"
 #include "tma.cuh"
 
@@ -442,16 +443,59 @@ constexpr int rows_per_tile(int n) {
     return r;
 }
 
-// State an engine keeps per thread: register twiddles (0), the DFT-16 fragments (1), nothing (2).
+// State an engine keeps per thread: register twiddles (0), the DFT-16 fragments (1), nothing (2), the tcgen05 block
+// state (3).
 template <int N, int ENG>
-using EngineState = std::conditional_t<ENG == 0, TwRegs<N>, std::conditional_t<ENG == 1, Dft16Frags, int>>;
+using EngineState = std::conditional_t<ENG == 0, TwRegs<N>,
+                                       std::conditional_t<ENG == 1, Dft16Frags, std::conditional_t<ENG == 3, Tc5, int>>>;
+
+// The tcgen05 engine (3) takes lines of 256 and 512 points in tiles of whole 128-vector blocks.
+constexpr bool tc5_tile(int n, int lines) { return (n == 256 || n == 512) && (n * lines) % 2048 == 0; }
+constexpr int tc5_blocks(int n, int lines) { return n * lines / 2048; }
+
+// Engine 3's set-up, by every thread of the block: tensor memory (warp 0), the B matrices, the MMA barrier.
+template <int MB>
+__device__ __forceinline__ Tc5 tc5_setup(uint8_t* area, uint32_t* tmem_slot, uint64_t* mma_bar, int tid, int nthreads) {
+    if (tid < 32) tmem_alloc(tmem_slot, tc5_tmem_cols(MB));
+    tc5_build_b(area + (size_t)MB * 3 * kTc5Plane, tid, nthreads);
+    if (tid == 0) {
+        mbar_init(mma_bar, 1);
+        fence_barrier_init();
+    }
+    fence_proxy_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    Tc5 c;
+    c.a_ptr = area;
+    c.a_base = smem_u32(area);
+    c.b_base = c.a_base + (uint32_t)MB * 3u * kTc5Plane;
+    c.tmem = *tmem_slot;
+    c.bar = mma_bar;
+    c.phase = 0;
+    return c;
+}
+
+// Engine 3's release: after every thread's last tensor-memory access (and, when a wait ran out, one more bounded
+// wait for the products in flight), warp 0 frees the columns.
+template <int MB>
+__device__ __forceinline__ void tc5_release(const Tc5& c, int tid, bool aborted) {
+    tc_fence_before();
+    __syncthreads();
+    if (aborted && tid == 0) mbar_wait_bounded(c.bar, c.phase ^ 1u, kTc5WaitPolls);
+    __syncthreads();
+    if (tid < 32) {
+        tc_fence_after();
+        tmem_dealloc(c.tmem, tc5_tmem_cols(MB));
+    }
+}
 
 // Blocks per SM the engines ask the compiler for. The tensor-core engine: two when a block has at most 256 threads
 // (at most 128 registers a thread). The float32 register engine: three for its 256-thread blocks (at most 85
 // registers; 512^2 fits without spills and gains a third block per SM). The float32 shared-memory engine keeps the
 // compiler's choice (capped at 84 registers it spilled and lost 12 % at 768^2).
 constexpr int tc_min_blocks(int threads, int eng) {
-    if (eng == 1) return threads <= 256 ? 2 : 1;
+    if (eng == 1 || eng == 3) return threads <= 256 ? 2 : 1;
     if (eng == 0) return threads == 256 ? 3 : 1;
     return 1;
 }
@@ -471,6 +515,8 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     constexpr uint32_t STAGE_BYTES = 2u * TILE * sizeof(float2);
     __shared__ __align__(8) uint64_t full[2];
     __shared__ int abort_flag;
+    __shared__ uint32_t tmem_slot;
+    __shared__ __align__(8) uint64_t mma_bar;
     float2* stages = reinterpret_cast<float2*>(smem_tma);
     const int c = threadIdx.x;
     const unsigned t = threadIdx.y;
@@ -487,6 +533,9 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     [[maybe_unused]] EngineState<N, ENG> eng;
     if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
+    else if constexpr (ENG == 3)
+        eng = tc5_setup<tc5_blocks(N, TC)>(smem_tma + 4 * (size_t)TILE * sizeof(float2), &tmem_slot, &mma_bar, tid,
+                                           TC * T);
     auto issue = [&](unsigned tile, int s) {
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
@@ -508,16 +557,15 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         const unsigned next = tile + gridDim.x;
         if (tid == 0) {
             // the previous tile's TMA store must have read its shared-memory source (a stage or the scratch tile)
-            // before the next copy into a stage and before this tile's transforms write the scratch tile
+            // before the next copy into a stage and before this tile's transforms write the scratch tile; after an
+            // abandoned tile no further copy starts, and the one in flight is waited for
             bulk_wait_read();
-            if (next < ntiles) issue(next, s ^ 1);
-            stage_wait(full, s, it, next < ntiles, err, &abort_flag);
+            const bool more = !abort_flag && next < ntiles;
+            if (more) issue(next, s ^ 1);
+            stage_wait(full, s, it, more, err, &abort_flag);
         }
         __syncthreads();
-        if (abort_flag) {
-            if (tid == 0) bulk_wait_all();
-            return;
-        }
+        if (abort_flag) break;
         const int b = (int)(tile / tiles_per_wave);
         const int iy = (int)(tile - (unsigned)b * tiles_per_wave) * TC + c;
         const float2* store_src = buf;  // where the finished tile lies in its natural layout
@@ -554,6 +602,27 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
 #pragma unroll
             for (int i = 0; i < 8; ++i) out[(t + T * i) * TC + c] = v[i];
             store_src = out;
+        } else if constexpr (ENG == 3) {
+            constexpr int NV = N / 16;
+            float2 z[8];
+            int ln, i0;
+            bool ok = tc5_fft<N, TC, true, -1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid, z, ln, i0);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int o = (i0 + NV * i) * TC + ln;
+                buf[o] = cmul(z[i], pbuf[o]) * pscale;
+            }
+            if constexpr (MODE == 0) {
+                __syncthreads();  // the spectrum times P is in the stage: the inverse transform gathers from it
+                ok = tc5_fft<N, TC, true, +1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid, z, ln, i0) && ok;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) buf[(i0 + NV * i) * TC + ln] = z[i];
+            }
+            if (!ok) {
+                atomicExch(err, 1);
+                abort_flag = 1;
+            }
+            store_src = buf;
         } else {
             using L = TileLayout<N, TC, true>;
             float2* scratch = stages + 4 * TILE;
@@ -589,6 +658,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
         }
     }
     if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
+    if constexpr (ENG == 3) tc5_release<tc5_blocks(N, TC)>(eng, tid, abort_flag != 0);
 }
 
 // rows: tile = RB consecutive rows of one wave (nx % RB == 0); a stage holds those RB rows and the RB rows of t.
@@ -603,6 +673,8 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
     constexpr int TILE = N * RB;
     __shared__ __align__(8) uint64_t full[2];
     __shared__ int abort_flag;
+    __shared__ uint32_t tmem_slot;
+    __shared__ __align__(8) uint64_t mma_bar;
     float2* stages = reinterpret_cast<float2*>(smem_rtma);
     const unsigned t = threadIdx.x;
     const int rr = threadIdx.y;
@@ -620,11 +692,15 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
     [[maybe_unused]] EngineState<N, ENG> eng;
     if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
+    else if constexpr (ENG == 3)
+        eng = tc5_setup<tc5_blocks(N, RB)>(smem_rtma + 4 * (size_t)TILE * sizeof(float2), &tmem_slot, &mma_bar, tid,
+                                           RB * T);
+    constexpr bool kStoreFromStage = (ENG == 0 || ENG == 3);  // the finished rows go back by a bulk store
     auto issue = [&](int tile, int s) {
         float2* dst = stages + s * 2 * TILE;
         const int row0 = tile * RB;
-        // ENG 0 stores each tile from its stage: the previous tile's store must have read the stage first
-        if constexpr (ENG == 0) bulk_wait_read();
+        // ENG 0 and 3 store each tile from its stage: the previous tile's store must have read the stage first
+        if constexpr (kStoreFromStage) bulk_wait_read();
         mbar_arrive_expect_tx(&full[s], with_t ? 2 * bytes : bytes);
         bulk_load(dst, psi + (size_t)row0 * N, bytes, &full[s]);
         if (with_t) {
@@ -640,16 +716,12 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
         const float2* tbuf = buf + TILE;
         const int next = tile + gridDim.x;
         if (tid == 0) {
-            if (next < ntiles) issue(next, s ^ 1);
-            stage_wait(full, s, it, next < ntiles, err, &abort_flag);
+            const bool more = !abort_flag && next < ntiles;  // after an abandoned tile no further copy starts
+            if (more) issue(next, s ^ 1);
+            stage_wait(full, s, it, more, err, &abort_flag);
         }
         __syncthreads();
-        if (abort_flag) {
-            if constexpr (ENG == 0) {
-                if (tid == 0) bulk_wait_all();
-            }
-            return;
-        }
+        if (abort_flag) break;
         float2* row = psi + (size_t)(tile * RB + rr) * N;
         if constexpr (ENG == 0) {
             float2 v[8];
@@ -670,6 +742,40 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
             // barrier below
 #pragma unroll
             for (int i = 0; i < 8; ++i) buf[rr * N + t + T * i] = v[i];
+        } else if constexpr (ENG == 3) {
+            constexpr int NV = N / 16;
+            float2 z[8];
+            int ln, i0;
+            bool ok = true;
+            if (inv) {
+                ok = tc5_fft<N, RB, false, +1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid, z, ln, i0);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int o = ln * N + i0 + NV * i;
+                    buf[o] = with_t ? cmul(z[i], tbuf[o]) * scale : z[i] * scale;
+                }
+                if (fwd) {
+                    __syncthreads();  // the rows times t are in the stage: the forward transform gathers from them
+                    ok = tc5_fft<N, RB, false, -1, PRE_NONE>(buf, nullptr, 1.0f, tw, eng, tid, z, ln, i0) && ok;
+                }
+            } else if (fwd) {
+                if (with_t) ok = tc5_fft<N, RB, false, -1, PRE_MUL>(buf, tbuf, scale, tw, eng, tid, z, ln, i0);
+                else ok = tc5_fft<N, RB, false, -1, PRE_SCALE>(buf, nullptr, scale, tw, eng, tid, z, ln, i0);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int o = rr * N + (int)t + T * i;
+                    buf[o] = with_t ? cmul(buf[o], tbuf[o]) * scale : buf[o] * scale;
+                }
+            }
+            if (fwd) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) buf[ln * N + i0 + NV * i] = z[i];
+            }
+            if (!ok) {
+                atomicExch(err, 1);
+                abort_flag = 1;
+            }
         } else if constexpr (ENG == 2) {
             using L = CcLayout<N, RB, false>;
             float2* scratch = stages + 4 * TILE;
@@ -719,16 +825,17 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
         }
         fence_proxy_async_shared();
         __syncthreads();  // every thread is done with the stage before its next copy
-        if constexpr (ENG == 0) {
+        if constexpr (kStoreFromStage) {
             if (tid == 0) {
                 bulk_store(psi + (size_t)tile * RB * N, buf, bytes);
                 bulk_commit();
             }
         }
     }
-    if constexpr (ENG == 0) {
+    if constexpr (kStoreFromStage) {
         if (tid == 0) bulk_wait_all();  // the stores read this block's shared memory: finish them before it is freed
     }
+    if constexpr (ENG == 3) tc5_release<tc5_blocks(N, RB)>(eng, tid, abort_flag != 0);
 }
 
 // ---- plans and launches ---------------------------------------------------------------------------------------------
@@ -868,19 +975,35 @@ void ensure_err_flag(Context& ctx) {
     if (ctx.sm_count == 0) SIMK_CUDA(cudaDeviceGetAttribute(&ctx.sm_count, cudaDevAttrMultiProcessorCount, ctx.device));
 }
 
+// Dynamic shared memory of a TMA pass: two stages of (wave tile, t or P tile), plus the shared-memory engines' scratch
+// tile (1, 2) or the tcgen05 engine's operands (3).
+constexpr size_t tma_pass_smem(int n, int lines, int eng) {
+    return eng == 3 ? 4 * (size_t)n * lines * sizeof(float2) + tc5_smem_bytes(tc5_blocks(n, lines))
+                    : (eng != 0 ? 5 : 4) * (size_t)n * lines * sizeof(float2);
+}
+
+// Blocks per SM of a persistent pass: the occupancy, and for the tcgen05 engine at most what tensor memory holds.
+inline int pass_blocks_per_sm(int occupancy, int eng, int mb) {
+    if (eng == 3) occupancy = std::min(occupancy, 512 / (int)tc5_tmem_cols(mb));
+    return occupancy;
+}
+
 template <int N, int ENG>
 bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
                      int fwd, float scale) {
     constexpr int T = N / 8;
     constexpr int RB = rows_per_tile(N);
+    if constexpr (ENG == 3 && !tc5_tile(N, RB)) {
+        return false;
+    } else {
     if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
-    // two stages of (rows, t rows), plus the shared-memory engines' scratch tile
-    const size_t smem = (ENG != 0 ? 5 : 4) * (size_t)N * RB * sizeof(float2);
+    const size_t smem = tma_pass_smem(N, RB, ENG);
     auto kern = fused_rows_tma<N, RB, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, RB * T, smem));
+        blocks_per_sm = pass_blocks_per_sm(blocks_per_sm, ENG, ENG == 3 ? tc5_blocks(N, RB) : 0);
     }
     if (blocks_per_sm <= 0) return false;
     ensure_err_flag(ctx);
@@ -891,19 +1014,23 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
+    }
 }
 
 template <int N, int TC, int MODE, int ENG>
 bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     constexpr int T = N / 8;
     constexpr int BOXH = tma_box_rows(N);
-    // two stages of (wave tile, P tile), plus the shared-memory engines' scratch tile
-    const size_t smem = (ENG != 0 ? 5 : 4) * (size_t)N * TC * sizeof(float2);
+    if constexpr (ENG == 3 && !tc5_tile(N, TC)) {
+        return false;
+    } else {
+    const size_t smem = tma_pass_smem(N, TC, ENG);
     auto kern = fused_cols_tma<N, TC, MODE, ENG>;
     static int blocks_per_sm = -1;
     if (blocks_per_sm < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, TC * T, smem));
+        blocks_per_sm = pass_blocks_per_sm(blocks_per_sm, ENG, ENG == 3 ? tc5_blocks(N, TC) : 0);
     }
     if (blocks_per_sm <= 0) return false;
     ensure_err_flag(ctx);
@@ -929,6 +1056,7 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
+    }
 }
 
 template <int N, int TC, int ENG = 0>
@@ -1012,6 +1140,10 @@ bool cols_ct(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
 // ---- the bf16x3 form: the same TMA passes with tensor-core line FFTs ---------------------------------------------------
 bool rows_tc(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv, int fwd,
              float scale) {
+    if (ctx.tcgen05) {  // the tcgen05 engine where its tiles fit, else the mma.sync engine
+        if (p.n == 256 && launch_rows_tma<256, 3>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return true;
+        if (p.n == 512 && launch_rows_tma<512, 3>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return true;
+    }
     switch (p.n) {
         case 256: return launch_rows_tma<256, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
         case 512: return launch_rows_tma<512, 1>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
@@ -1046,7 +1178,22 @@ bool cols_tc_n(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int 
     return false;
 }
 
+// The tcgen05 engine's column tiles are whole 128-vector blocks: 8 columns at 256, 4 or 8 at 512.
+template <int N>
+bool cols_tc5(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    if constexpr (N == 512) {
+        if (ctx.col_tile == 8 && launch_cols_tma<512, 8, 3>(ctx, p, a, count)) return true;
+        return launch_cols_tma<512, 4, 3>(ctx, p, a, count);
+    } else {
+        return launch_cols_tma<N, 8, 3>(ctx, p, a, count);
+    }
+}
+
 bool cols_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    if (ctx.tcgen05) {
+        if (p.n == 256 && cols_tc5<256>(ctx, p, a, count)) return true;
+        if (p.n == 512 && cols_tc5<512>(ctx, p, a, count)) return true;
+    }
     int tc = ctx.col_tile > 0 ? ctx.col_tile : 4;
     switch (p.n) {
         case 256: return cols_tc_n<256>(ctx, p, a, count, tc);
@@ -1235,6 +1382,7 @@ int propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, 
     key_append(key, ctx.form);
     key_append(key, ctx.col_tile);
     key_append(key, ctx.tma);
+    key_append(key, ctx.tcgen05);
     key_append(key, ctx.stream);
     const FusedDetect nodet{};
     const FusedDetect& d = det ? *det : nodet;
@@ -1350,7 +1498,7 @@ void scan_fused_batch(Context& ctx, PotentialImpl& pot, const simk_probe& probe,
     const long long N = g.count();
     // channel detectors are summed in the last column pass when it runs on the TMA passes (at most 64 channels)
     FusedDetect fd{};
-    const bool fuse = dplan.n_channels > 0 && dplan.n_channels <= 64 && ctx.tma;
+    const bool fuse = dplan.n_channels > 0 && dplan.n_channels <= 64 && ctx.tma && ctx.epilogue_detect;
     if (fuse) {
         ctx.det_partial.ensure((size_t)b * (g.ny / 2) * dplan.n_channels * sizeof(double));
         fd.plan = &dplan;

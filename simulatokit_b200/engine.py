@@ -20,12 +20,15 @@ class ExecutionOptions:
     may hold (default 1 GiB). graphs: capture each batch's slice loop in a CUDA graph. col_tile: columns per CTA of
     the fused column pass (0 = automatic). tma: the TMA-pipelined persistent column pass where available. autotune:
     time the column tile, TMA passes and batch size on the first fused scan of a grid and use the fastest where the
-    settings above are automatic."""
+    settings above are automatic. tcgen05: the bf16x3 form's DFT stages on the fifth-generation tensor cores
+    (tcgen05.mma, tensor-memory accumulators) at grid sides 256 and 512; False keeps the warp-level mma.sync stages.
+    epilogue_detect: sum the channel detectors inside the last column pass (TMA passes) instead of separate kernels."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
     def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
-                 col_tile: int = 0, tma: bool = True, autotune: bool = False):
+                 col_tile: int = 0, tma: bool = True, autotune: bool = False, tcgen05: bool = True,
+                 epilogue_detect: bool = True):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
         self.form = form
@@ -35,6 +38,8 @@ class ExecutionOptions:
         self.col_tile = int(col_tile)
         self.tma = bool(tma)
         self.autotune = bool(autotune)
+        self.tcgen05 = bool(tcgen05)
+        self.epilogue_detect = bool(epilogue_detect)
 
     @staticmethod
     def standard() -> "ExecutionOptions":
@@ -79,6 +84,8 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COL_TILE, o.col_tile))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TMA, 1 if o.tma else 0))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_AUTOTUNE, 1 if o.autotune else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TCGEN05, 1 if o.tcgen05 else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_EPILOGUE_DETECT, 1 if o.epilogue_detect else 0))
 
     def set_stream(self, stream_ptr: int | None):
         L.check(self.lib.simk_context_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))

@@ -1,9 +1,10 @@
 """The bf16x3 form against the float64 oracle.
 
-The form runs the fused TMA passes with each line FFT's radix-16 stages as tensor-core products of 3-term split-BF16
-operands with float32 accumulation (radix 2/3/4/8 first stage and twiddles in float32). Its bound is the one stated
-for this form: <= 1e-4 relative L2 against the float64 oracle on every detector image, and on the exit wave; the
-measured errors are printed. Grid sides it covers: 256, 512, 768, 1024, 2048.
+The form runs the fused TMA passes with each line FFT's radix-16 stages as tensor-core products of split-BF16 operands
+with float32 accumulation (radix 2/3/4/8 first stage and twiddles in float32): on the fifth-generation tensor cores
+(tcgen05.mma, data in three BF16 terms) at grid sides 256 and 512, and with warp-level mma.sync (data in two terms)
+at 768, 1024 and 2048 or when the tcgen05 option is off. Its bound is the one stated for this form: <= 1e-4 relative
+L2 against the float64 oracle on every detector image, and on the exit wave; the measured errors are printed.
 """
 
 import numpy as np
@@ -21,24 +22,28 @@ def engine():
     return sk.Engine.require()
 
 
-def _opts(form="bf16x3"):
-    return sk.ExecutionOptions(form=form)
+def _opts(form="bf16x3", tcgen05=True):
+    return sk.ExecutionOptions(form=form, tcgen05=tcgen05)
 
 
-def test_hrtem_srtio3_exit_wave(engine):
-    """SrTiO3 4x4x5, 256^2, 10 slices of 1.9525 A, 200 keV plane wave."""
+@pytest.mark.parametrize("tcgen05", [True, False])
+def test_hrtem_srtio3_exit_wave(engine, tcgen05):
+    """SrTiO3 4x4x5, 256^2, 10 slices of 1.9525 A, 200 keV plane wave, on either tensor-core engine."""
     s = O.srtio3_cell().repeated(4, 4, 5)
     op = O.Potential.from_structure(s, 256, 256, slice_thickness=1.9525)
     og = op.grid
     ts = [O.transmission(v, 200e3, og) for v in op.build()]
     ref = O.multislice(O.plane_wave(og), ts, op.thicknesses, 200e3, og)[-1]
     pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), 256, 256, slice_thickness=1.9525)
-    ex = sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), pot.grid), pot, options=_opts(),
+    ex = sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), pot.grid), pot, options=_opts(tcgen05=tcgen05),
                            engine=engine)[-1]
     e_wave = O.rel_l2(ex.field, ref)
     e_int = O.rel_l2(np.abs(ex.field) ** 2, np.abs(ref) ** 2)
-    print(f"bf16x3 HRTEM 256^2 x 10 slices: exit wave rel-L2 {e_wave:.2e}, intensity {e_int:.2e}")
+    print(f"bf16x3 ({'tcgen05' if tcgen05 else 'mma.sync'}) HRTEM 256^2 x 10 slices: exit wave rel-L2 {e_wave:.2e}, "
+          f"intensity {e_int:.2e}")
     assert e_wave <= 1e-4 and e_int <= 1e-4
+    if tcgen05:  # three-term data split: float32-like accuracy
+        assert e_wave <= 1e-5
 
 
 def _scan_vs_oracle(engine, cells, n, positions_per_side, dets_sk, dets_o, slice_thickness=3.905):
@@ -76,6 +81,7 @@ def test_stem_scan_512_full_cell(engine):
                             O.DetectorSpec("annular", {"inner": 50, "outer": 200})])
     print("512^2 rel-L2 vs float64 oracle (BF, HAADF):", errs)
     assert max(errs["bf16x3"]) <= 1e-4
+    assert max(errs["fused"]) <= 1e-4
 
 
 def test_probe_exit_wave_768(engine):
