@@ -61,6 +61,11 @@ extern "C" {
  * the k-space waves are neither written nor read back unless a pixelated or binned detector wants them; 0 = detect
  * from the stored waves with separate kernels. Default 1. */
 #define SIMK_OPT_EPILOGUE_DETECT 13
+/* The generator of simk_poisson_noise[_device]: 0 (default) = a generator of its own for every value and sample (the
+ * work splits over the GPU; a seed gives the same noise on every run, not the reference's draws); 1 = the reference's
+ * single GaussianGenerator stream over the samples and values in order (ScanOperations.swift:80-117), walked by one
+ * device thread, so a seed gives the reference's draws. */
+#define SIMK_OPT_POISSON_STREAM 14
 
 /* ---- Lobato pi choice (LobatoParameterization.PiConstant, LobatoParameterization.swift:15-24) ---- */
 #define SIMK_PI_EXACT 0
@@ -293,7 +298,8 @@ int simk_gaussian_source_size_device(simk_context* ctx, int32_t nx, int32_t ny, 
  * out[s count + i] ~ Poisson(max(in[i] dose, 0)), by the reference's sampler (Knuth below a mean of 10, PTRS above).
  * poissonNoise(dosePerArea:samplingX:samplingY:...) is dose = samplingX samplingY dosePerArea. The generator differs
  * from the reference's single stream: every value and sample has its own xoshiro256** seeded by
- * mix(mix(seed) + s count + i), so a seed gives the same noise on every run, not the reference's draws. dose finite
+ * mix(mix(seed) + s count + i), so a seed gives the same noise on every run, not the reference's draws (with
+ * SIMK_OPT_POISSON_STREAM = 1 the reference's stream instead, drawn in order by one device thread). dose finite
  * and >= 0, samples >= 1, finite values, else SIMK_ERR_INVALID. `out` (samples x count) may equal `in` when samples is
  * 1. */
 int simk_poisson_noise(simk_context* ctx, int64_t count, const double* in, double dose, int32_t samples, uint64_t seed,

@@ -79,10 +79,17 @@ __global__ void k_scatter(double2* D, const int* pix, const double* w, int count
         D[pix[i]] = make_double2(w[i], 0.0);
 }
 
-__global__ void k_accum_spectrum(double2* S, const double2* D, const double* K, long long N) {
+// S += sum over the `count` spectra D_q (N apart) of D_q K_{elem[q]}, the elements in the given (increasing Z) order, so
+// each pixel sees the same sequence of additions as one element at a time.
+__global__ void k_accum_spectra(double2* S, const double2* D, const double* K, const int* elem, int count, long long N) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-        const double k = K[i];
-        S[i] = make_double2(S[i].x + D[i].x * k, S[i].y + D[i].y * k);
+        double2 s = S[i];
+        for (int q = 0; q < count; ++q) {
+            const double k = K[(long long)elem[q] * N + i];
+            const double2 d = D[(long long)q * N + i];
+            s = make_double2(s.x + d.x * k, s.y + d.y * k);
+        }
+        S[i] = s;
     }
 }
 
@@ -244,22 +251,40 @@ void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice,
     }
     SIMK_CUDA(cudaGetLastError());
     pot.V.alloc(std::max<long long>(1, S) * N * sizeof(double));
-    DeviceBuffer spec(N * sizeof(double2)), delta(N * sizeof(double2));
+    // the elements present in a slice are transformed together, up to `chunk` delta images (256 MiB) per batch
+    const int chunk = (int)std::max<long long>(1, std::min<long long>(E, (256LL << 20) / (N * (long long)sizeof(double2))));
+    DeviceBuffer spec(N * sizeof(double2)), delta((size_t)chunk * N * sizeof(double2));
+    DeviceBuffer d_elem((size_t)std::max(1, S * E) * sizeof(int));
+    std::vector<int> present;  // per slice, the elements with atoms in it, in increasing Z; concatenated over slices
+    std::vector<int> present_ptr(1, 0);
+    for (int j = 0; j < S; ++j) {
+        for (int e = 0; e < E; ++e)
+            if (group_ptr[j * E + e + 1] > group_ptr[j * E + e]) present.push_back(e);
+        present_ptr.push_back((int)present.size());
+    }
+    if (!present.empty())
+        SIMK_CUDA(cudaMemcpyAsync(d_elem.ptr, present.data(), present.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                  ctx.stream));
     const LinePlan& prow = ctx.plan(g.ny, 64);
     const LinePlan& pcol = ctx.plan(g.nx, 64);
     for (int j = 0; j < S; ++j) {
         k_zero_d2<<<blocks_for(N), 256, 0, ctx.stream>>>(spec.as<double2>(), N);
         ++ctx.launches;
-        for (int e = 0; e < E; ++e) {
-            long long a0 = group_ptr[j * E + e], a1 = group_ptr[j * E + e + 1];
-            if (a1 == a0) continue;
-            k_zero_d2<<<blocks_for(N), 256, 0, ctx.stream>>>(delta.as<double2>(), N);
-            k_scatter<<<blocks_for(a1 - a0), 256, 0, ctx.stream>>>(delta.as<double2>(), d_pix.as<int>() + a0,
-                                                                    d_w.as<double>() + a0, (int)(a1 - a0));
-            ctx.launches += 2;
-            fft2(prow, pcol, delta.ptr, g.nx, g.ny, 1, -1, 1.0, ctx.stream, &ctx.launches);
-            k_accum_spectrum<<<blocks_for(N), 256, 0, ctx.stream>>>(spec.as<double2>(), delta.as<double2>(),
-                                                                     kern.as<double>() + e * N, N);
+        for (int q0 = present_ptr[j]; q0 < present_ptr[j + 1]; q0 += chunk) {
+            const int nq = std::min(chunk, present_ptr[j + 1] - q0);
+            k_zero_d2<<<blocks_for((long long)nq * N), 256, 0, ctx.stream>>>(delta.as<double2>(), (long long)nq * N);
+            ++ctx.launches;
+            for (int q = 0; q < nq; ++q) {
+                const int e = present[q0 + q];
+                const long long a0 = group_ptr[j * E + e], a1 = group_ptr[j * E + e + 1];
+                k_scatter<<<blocks_for(a1 - a0), 256, 0, ctx.stream>>>(delta.as<double2>() + (long long)q * N,
+                                                                        d_pix.as<int>() + a0, d_w.as<double>() + a0,
+                                                                        (int)(a1 - a0));
+                ++ctx.launches;
+            }
+            fft2(prow, pcol, delta.ptr, g.nx, g.ny, nq, -1, 1.0, ctx.stream, &ctx.launches);
+            k_accum_spectra<<<blocks_for(N), 256, 0, ctx.stream>>>(spec.as<double2>(), delta.as<double2>(),
+                                                                    kern.as<double>(), d_elem.as<int>() + q0, nq, N);
             ++ctx.launches;
         }
         fft2(prow, pcol, spec.ptr, g.nx, g.ny, 1, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);

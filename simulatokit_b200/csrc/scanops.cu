@@ -269,6 +269,26 @@ __global__ void k_poisson(const double* __restrict__ in, double* __restrict__ ou
     }
 }
 
+// The reference's own stream (ScanOperations.swift:80-117): one generator seeded by `seed`, every sample's values drawn
+// in order, so that a seed gives the reference's draws. The number of uniforms a draw takes depends on the draws, so
+// the chain cannot be split: one thread walks it. err bits as k_poisson.
+__global__ void k_poisson_sequential(const double* __restrict__ in, double* __restrict__ out, long long count,
+                                     int samples, double dose, uint64_t seed, int* err) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    Xoshiro g;
+    seed_xoshiro(g, seed);
+    for (int s = 0; s < samples; ++s)
+        for (long long i = 0; i < count; ++i) {
+            const double m = __dmul_rn(in[i], dose);
+            if (!isfinite(m)) {
+                atomicOr(err, 2);
+                out[(long long)s * count + i] = 0.0;
+                continue;
+            }
+            out[(long long)s * count + i] = poisson_draw(m > 0.0 ? m : 0.0, g, err);
+        }
+}
+
 // ---- integrated gradient --------------------------------------------------------------------------------------------
 
 __global__ void k_gradient_load(const double* __restrict__ gx, const double* __restrict__ gy, long long stride,
@@ -433,8 +453,11 @@ void poisson_noise_device(Context& ctx, long long count, const double* in, doubl
     SIMK_CUDA(cudaMemsetAsync(ctx.post_flag.ptr, 0, sizeof(int), ctx.stream));
     {
         KernelTimer t(ctx, "poisson", 8.0 * (double)count + 8.0 * (double)count * samples);
-        k_poisson<<<blocks_for(count), 256, 0, ctx.stream>>>(in, out, count, samples, dose, seed,
-                                                             ctx.post_flag.as<int>());
+        if (ctx.poisson_stream == 1)
+            k_poisson_sequential<<<1, 1, 0, ctx.stream>>>(in, out, count, samples, dose, seed, ctx.post_flag.as<int>());
+        else
+            k_poisson<<<blocks_for(count), 256, 0, ctx.stream>>>(in, out, count, samples, dose, seed,
+                                                                 ctx.post_flag.as<int>());
     }
     ++ctx.launches;
     SIMK_CUDA(cudaGetLastError());

@@ -225,11 +225,14 @@ class ScanMeasurement:
 
     def poissonNoise(self, dose: float | None = None, *, dosePerArea: float | None = None,
                      samplingX: float | None = None, samplingY: float | None = None, samples: int | None = None,
-                     seed: int = 0, engine: Engine | None = None):
+                     seed: int = 0, stream: str = "values", engine: Engine | None = None):
         """Poisson noise for a total dose [electrons per pattern] or a dose per area [electrons / A^2] over scan pixels
         of samplingX x samplingY [A] (ScanOperations.swift:74-127): every value times the dose, clipped at 0, one
         Poisson draw each. With `samples`, a list of that many independent draws. A seed gives the same noise on every
-        run; every value has a generator of its own (the reference's draws come from one stream)."""
+        run. stream="values" (default): every value has a generator of its own, drawn in parallel; stream="reference":
+        the reference's single generator stream in value order (one device thread), so a seed gives its draws."""
+        if stream not in ("values", "reference"):
+            _refuse(f"unknown Poisson stream {stream!r}: 'values' or 'reference'")
         if dosePerArea is not None:
             if dose is not None:
                 _refuse("give dose or dosePerArea, not both")
@@ -249,8 +252,12 @@ class ScanMeasurement:
             _refuse(f"the dose must be finite and non-negative, got {dose}")
         e = engine or Engine.require()
         out = np.empty(n_samples * vin.size)
-        L.check(e.lib.simk_poisson_noise(e.handle, vin.size, L.dptr(vin), float(dose), n_samples,
-                                         int(seed) & 0xFFFFFFFFFFFFFFFF, L.dptr(out)))
+        L.check(e.lib.simk_context_set_option(e.handle, L.OPT_POISSON_STREAM, 1 if stream == "reference" else 0))
+        try:
+            L.check(e.lib.simk_poisson_noise(e.handle, vin.size, L.dptr(vin), float(dose), n_samples,
+                                             int(seed) & 0xFFFFFFFFFFFFFFFF, L.dptr(out)))
+        finally:
+            L.check(e.lib.simk_context_set_option(e.handle, L.OPT_POISSON_STREAM, 0))
         draws = [ScanMeasurement(list(self.scan_shape), list(self.value_shape),
                                  out[s * vin.size:(s + 1) * vin.size].reshape(np.shape(self.values)))
                  for s in range(n_samples)]

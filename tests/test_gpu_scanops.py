@@ -103,6 +103,25 @@ def test_poisson_noise_is_the_oracles_per_value_streams(engine):
     assert np.array_equal(single.values, want[0])
 
 
+def test_poisson_noise_in_the_reference_order_is_the_references_stream(engine):
+    """stream="reference": one GaussianGenerator over every sample and value in order (ScanOperations.swift:80-117),
+    bit-equal to the oracle's restatement of that loop, so a seed gives the reference's own draws; the samples
+    continue one stream, so sample 0 is the single draw of the same seed."""
+    rng = np.random.default_rng(10)
+    v = np.concatenate([rng.random(120) * 3.0, 3.0 + rng.random(120) * 400.0, [0.0, -2.0, 10.0 / 3.0, 1e4]])
+    m = sk.ScanMeasurement([len(v), 1], [], v)
+    draws = m.poissonNoise(3.0, samples=3, seed=2024, stream="reference", engine=engine)
+    want = O.poisson_noise_sequential(v, 3.0, 2024, samples=3)
+    for s in range(3):
+        assert np.array_equal(draws[s].values, want[s])
+    single = m.poissonNoise(3.0, seed=2024, stream="reference", engine=engine)
+    assert np.array_equal(single.values, want[0])
+    # the default per-value streams are untouched by the option (it is reset after the call)
+    assert np.array_equal(m.poissonNoise(3.0, seed=123, engine=engine).values, O.poisson_noise_streams(v, 3.0, 123)[0])
+    with pytest.raises(sk.InvalidArgument):
+        m.poissonNoise(3.0, seed=1, stream="other", engine=engine)
+
+
 @pytest.mark.parametrize("mean", [0.5, 4.0, 9.9, 10.0, 37.0, 800.0])
 def test_poisson_noise_has_the_poisson_mean_and_variance(engine, mean):
     n = 20000
