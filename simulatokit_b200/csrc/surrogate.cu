@@ -9,9 +9,12 @@
 // summed potential. Network: 18 -> 64 -> 64 -> 64 -> 1 with SiLU.
 // Training (on the device, by the kernels below): samples drawn uniformly in log rho, zl and the slab thickness inside
 // the trained domain, labelled by the float64 quadrature itself; each sample runs the network at both edges (rows b and
-// B + b of a doubled batch) and back-propagates +dF and -dF; mean-squared error; Adam. Every reduction runs in a fixed
-// order, so training is deterministic for a seed. Inference: tensor-core tiles of 16 queries per warp (k_sg_infer),
-// f16 weights and activations (SiLU in f16x2), float32 accumulation.
+// B + b of a doubled batch) and back-propagates +dF and -dF; mean-squared error; Adam. A training step is two launches:
+// k_sg_train runs the forward and backward pass of 32 samples per block with every contraction on the tensor cores
+// (mma.sync TF32, operands split in two terms: float32 accuracy) and writes the block's gradient; k_sg_reduce_adam adds
+// the blocks' gradients in block order and takes the Adam step. Every reduction runs in a fixed order, so training is
+// deterministic for a seed. Inference: tensor-core tiles of 16 queries per warp (k_sg_infer), f16 weights and
+// activations (SiLU in f16x2), float32 accumulation.
 //
 // Parameter layout (float32, kSurrogateParams values): emb[103][16] | W1[64][18] b1[64] | W2[64][64] b2[64] |
 // W3[64][64] b3[64] | W4[64] b4[1].
@@ -51,86 +54,280 @@ __host__ __device__ inline void surrogate_features(double rho, double z, float* 
     f[1] = (float)(asinh(z / rho) / 4.0);
 }
 
-// ---- training kernels (one output element per thread; reductions over the batch in order) ---------------------------
-__global__ void k_sg_x0(const int* __restrict__ z, const float* __restrict__ feats, const float* __restrict__ emb,
-                        int B, float* __restrict__ x0) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B * kIn; i += gridDim.x * blockDim.x) {
-        const int b = i / kIn, k = i % kIn;
-        x0[i] = (k < kEmbed) ? emb[(z[b] - 1) * kEmbed + k] : feats[b * 2 + (k - kEmbed)];
-    }
+// ---- training: one fused forward + backward per block of samples, on the tensor cores ----------------------------
+// A block takes kTrSamples samples: rows 0 .. kTrSamples - 1 are their upper-edge rows, the next kTrSamples their
+// lower-edge rows. Every contraction of the forward and backward pass is a warp-level tensor-core product
+// (mma.sync m16n8k8, TF32 operands split in two terms, x = x_hi + x_lo, with the three products hi hi + hi lo + lo hi:
+// float32 accuracy), from float32 operands in shared memory. The block writes the gradient of its samples for every
+// parameter to its own row of `partial`; k_sg_reduce_adam adds the rows in block order (fixed, so training is
+// deterministic for a seed) and takes the Adam step.
+constexpr int kTrSamples = 32;
+constexpr int kTrRows = 2 * kTrSamples;
+constexpr int kTrThreads = 256;
+constexpr int kTrWarps = kTrThreads / 32;
+constexpr int kIn8 = 24;          // layer-1 inputs padded to whole k-steps of 8
+constexpr int kLdH = kHidden + 4; // row pitch of [row][64] buffers (4 mod 32: conflict-free fragment loads)
+constexpr int kLd1 = kIn8 + 4;    // row pitch of [row][24] buffers
+// shared memory, in floats
+constexpr int kTrW1 = 0;                            // W1 [64][kLd1] (inputs 18 .. 23 zero)
+constexpr int kTrW2 = kTrW1 + kHidden * kLd1;       // W2 [64][kLdH]
+constexpr int kTrW3 = kTrW2 + kHidden * kLdH;       // W3 [64][kLdH]
+constexpr int kTrVec = kTrW3 + kHidden * kLdH;      // b1 b2 b3 W4 [64 each], b4
+constexpr int kTrX0 = kTrVec + 4 * kHidden + 4;     // X0 [rows][kLd1]
+constexpr int kTrA1 = kTrX0 + kTrRows * kLd1;       // pre-activations A1, A2, A3 [rows][kLdH]
+constexpr int kTrA2 = kTrA1 + kTrRows * kLdH;
+constexpr int kTrA3 = kTrA2 + kTrRows * kLdH;
+constexpr int kTrH = kTrA3 + kTrRows * kLdH;        // an activation SiLU(A) [rows][kLdH]
+constexpr int kTrD0 = kTrH + kTrRows * kLdH;        // gradients of the pre-activations [rows][kLdH], two buffers
+constexpr int kTrD1 = kTrD0 + kTrRows * kLdH;
+constexpr int kTrY = kTrD1 + kTrRows * kLdH;        // y [rows], dy [rows]
+constexpr int kTrDy = kTrY + kTrRows;
+constexpr int kTrZ = kTrDy + kTrRows;               // Z of every row (int)
+constexpr int kTrFloats = kTrZ + kTrRows;
+constexpr size_t kTrSmem = (size_t)kTrFloats * sizeof(float);
+
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+    uint32_t h, l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+    const float r = x - __uint_as_float(h);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
+    hi = h;
+    lo = l;
 }
 
-// Y[b][o] = b[o] + sum_i W[o][i] X[b][i]; with act, H = silu(Y) too.
-__global__ void k_sg_linear(const float* __restrict__ X, const float* __restrict__ W, const float* __restrict__ bias,
-                            int B, int in, int out, float* __restrict__ Y, float* __restrict__ H) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B * out; i += gridDim.x * blockDim.x) {
-        const int b = i / out, o = i % out;
-        float s = bias[o];
-        for (int k = 0; k < in; ++k) s += W[o * in + k] * X[b * in + k];
-        Y[i] = s;
-        if (H) H[i] = silu(s);
-    }
+__device__ __forceinline__ void mma_tf32_1688(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// rows b and B + b of y are C at the upper and the lower edge of sample b: F_hat = y[b] - y[B + b]
-__global__ void k_sg_loss(const float* __restrict__ y, const float* __restrict__ target, int B, float* __restrict__ dy,
-                          double* __restrict__ loss_terms) {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
-        const float e = (y[b] - y[B + b]) - target[b];
-        dy[b] = 2.0f * e / (float)B;
-        dy[B + b] = -2.0f * e / (float)B;
-        loss_terms[b] = (double)e * (double)e;
-    }
-}
-
-// dW[o][i] = sum_b dY[b][o] X[b][i]; db[o] = sum_b dY[b][o]
-__global__ void k_sg_grad_w(const float* __restrict__ dY, const float* __restrict__ X, int B, int in, int out,
-                            float* __restrict__ dW, float* __restrict__ db) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < out * (in + 1); i += gridDim.x * blockDim.x) {
-        const int o = i / (in + 1), k = i % (in + 1);
-        float s = 0.0f;
-        if (k < in) {
-            for (int b = 0; b < B; ++b) s += dY[b * out + o] * X[b * in + k];
-            dW[o * in + k] = s;
-        } else {
-            for (int b = 0; b < B; ++b) s += dY[b * out + o];
-            db[o] = s;
+// C[M][N] = sum_k A(m, k) B(k, n) over K, tiles of 16 x 8 spread over the block's warps; `store(m, n, value)` takes the
+// result. Fragments (g = lane / 4, q = lane % 4): A (g, q), (g + 8, q), (g, q + 4), (g + 8, q + 4); B (q, g),
+// (q + 4, g); C (g, 2q), (g, 2q + 1), (g + 8, 2q), (g + 8, 2q + 1).
+template <int M, int N, int K, typename FA, typename FB, typename FS>
+__device__ __forceinline__ void tr_gemm(FA a, FB b, FS store, int warp, int lane) {
+    constexpr int TN = N / 8, NT = (M / 16) * TN;
+    static_assert(M % 16 == 0 && N % 8 == 0 && K % 8 == 0, "tile shape");
+    const int g = lane >> 2, q = lane & 3;
+    for (int t = warp; t < NT; t += kTrWarps) {
+        const int m0 = (t / TN) * 16, n0 = (t % TN) * 8;
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 4
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            uint32_t ah[4], al[4], bh0, bl0, bh1, bl1;
+            tf32_split(a(m0 + g, k0 + q), ah[0], al[0]);
+            tf32_split(a(m0 + g + 8, k0 + q), ah[1], al[1]);
+            tf32_split(a(m0 + g, k0 + q + 4), ah[2], al[2]);
+            tf32_split(a(m0 + g + 8, k0 + q + 4), ah[3], al[3]);
+            tf32_split(b(k0 + q, n0 + g), bh0, bl0);
+            tf32_split(b(k0 + q + 4, n0 + g), bh1, bl1);
+            mma_tf32_1688(acc, al, bh0, bh1);
+            mma_tf32_1688(acc, ah, bl0, bl1);
+            mma_tf32_1688(acc, ah, bh0, bh1);
         }
+        store(m0 + g, n0 + 2 * q, acc[0]);
+        store(m0 + g, n0 + 2 * q + 1, acc[1]);
+        store(m0 + g + 8, n0 + 2 * q, acc[2]);
+        store(m0 + g + 8, n0 + 2 * q + 1, acc[3]);
     }
 }
 
-// dX[b][k] = sum_o dY[b][o] W[o][k], times silu'(A[b][k]) when A is given
-__global__ void k_sg_grad_x(const float* __restrict__ dY, const float* __restrict__ W, const float* __restrict__ A,
-                            int B, int in, int out, float* __restrict__ dX) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B * in; i += gridDim.x * blockDim.x) {
-        const int b = i / in, k = i % in;
-        float s = 0.0f;
-        for (int o = 0; o < out; ++o) s += dY[b * out + o] * W[o * in + k];
-        dX[i] = A ? s * silu_grad(A[i]) : s;
+// One forward and backward pass of samples [blockIdx.x kTrSamples, +kTrSamples) of a doubled batch of B samples (row b
+// and row B + b of z and feats: the upper and the lower edge of sample b): the per-block gradients into
+// partial[blockIdx.x][kSurrogateParams] and, with loss_terms, each sample's squared error.
+__global__ void __launch_bounds__(kTrThreads) k_sg_train(const float* __restrict__ params, const int* __restrict__ z,
+                                                         const float* __restrict__ feats,
+                                                         const float* __restrict__ target, int B,
+                                                         float* __restrict__ partial, double* __restrict__ loss_terms) {
+    extern __shared__ __align__(16) float sm_tr[];
+    float* W1 = sm_tr + kTrW1;
+    float* W2 = sm_tr + kTrW2;
+    float* W3 = sm_tr + kTrW3;
+    float* vec = sm_tr + kTrVec;  // b1 b2 b3 W4 b4
+    float* X0 = sm_tr + kTrX0;
+    float* A1 = sm_tr + kTrA1;
+    float* A2 = sm_tr + kTrA2;
+    float* A3 = sm_tr + kTrA3;
+    float* H = sm_tr + kTrH;
+    float* D0 = sm_tr + kTrD0;
+    float* D1 = sm_tr + kTrD1;
+    float* y = sm_tr + kTrY;
+    float* dy = sm_tr + kTrDy;
+    int* zr = reinterpret_cast<int*>(sm_tr + kTrZ);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int s0 = blockIdx.x * kTrSamples;
+    float* out = partial + (size_t)blockIdx.x * kSurrogateParams;
+    // ---- parameters and inputs ----
+    for (int i = tid; i < kHidden * kLd1; i += kTrThreads) {
+        const int n = i / kLd1, k = i % kLd1;
+        W1[i] = k < kIn ? params[OFF_W1 + n * kIn + k] : 0.0f;
     }
-}
-
-// dEmb[z][k] = sum over the batch's samples of element z of dX0[b][k]
-__global__ void k_sg_grad_emb(const float* __restrict__ dX0, const int* __restrict__ z, int B,
-                              float* __restrict__ demb) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 103 * kEmbed; i += gridDim.x * blockDim.x) {
+    for (int i = tid; i < kHidden * kHidden; i += kTrThreads) {
+        const int n = i / kHidden, k = i % kHidden;
+        W2[n * kLdH + k] = params[OFF_W2 + i];
+        W3[n * kLdH + k] = params[OFF_W3 + i];
+    }
+    for (int i = tid; i < kHidden; i += kTrThreads) {
+        vec[i] = params[OFF_B1 + i];
+        vec[kHidden + i] = params[OFF_B2 + i];
+        vec[2 * kHidden + i] = params[OFF_B3 + i];
+        vec[3 * kHidden + i] = params[OFF_W4 + i];
+    }
+    if (tid == 0) vec[4 * kHidden] = params[OFF_B4];
+    for (int i = tid; i < kTrRows * kLd1; i += kTrThreads) {
+        const int r = i / kLd1, k = i % kLd1;
+        const int smp = s0 + (r % kTrSamples);
+        const bool ok = smp < B;
+        const long long row = ok ? (r < kTrSamples ? smp : (long long)B + smp) : 0;
+        const int zz = ok ? z[row] : 1;
+        if (k == 0) zr[r] = ok ? zz : 0;
+        float v = 0.0f;
+        if (ok) {
+            if (k < kEmbed) v = params[OFF_EMB + (zz - 1) * kEmbed + k];
+            else if (k < kIn) v = feats[row * 2 + (k - kEmbed)];
+        }
+        X0[r * kLd1 + k] = v;
+    }
+    __syncthreads();
+    // ---- forward ----
+    const float* b1 = vec;
+    const float* b2 = vec + kHidden;
+    const float* b3 = vec + 2 * kHidden;
+    const float* w4 = vec + 3 * kHidden;
+    tr_gemm<kTrRows, kHidden, kIn8>([&](int m, int k) { return X0[m * kLd1 + k]; },
+                                    [&](int k, int n) { return W1[n * kLd1 + k]; },
+                                    [&](int m, int n, float v) {
+                                        const float a = v + b1[n];
+                                        A1[m * kLdH + n] = a;
+                                        H[m * kLdH + n] = silu(a);
+                                    },
+                                    warp, lane);
+    __syncthreads();
+    tr_gemm<kTrRows, kHidden, kHidden>([&](int m, int k) { return H[m * kLdH + k]; },
+                                       [&](int k, int n) { return W2[n * kLdH + k]; },
+                                       [&](int m, int n, float v) { A2[m * kLdH + n] = v + b2[n]; }, warp, lane);
+    __syncthreads();
+    for (int i = tid; i < kTrRows * kHidden; i += kTrThreads) {
+        const int m = i / kHidden, n = i % kHidden;
+        H[m * kLdH + n] = silu(A2[m * kLdH + n]);
+    }
+    __syncthreads();
+    tr_gemm<kTrRows, kHidden, kHidden>([&](int m, int k) { return H[m * kLdH + k]; },
+                                       [&](int k, int n) { return W3[n * kLdH + k]; },
+                                       [&](int m, int n, float v) { A3[m * kLdH + n] = v + b3[n]; }, warp, lane);
+    __syncthreads();
+    // output layer: y = b4 + sum_k silu(A3) W4, one warp per row, lanes over k, shuffle tree (fixed order)
+    for (int m = warp; m < kTrRows; m += kTrWarps) {
+        float sum = silu(A3[m * kLdH + lane]) * w4[lane] + silu(A3[m * kLdH + lane + 32]) * w4[lane + 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) y[m] = sum + vec[4 * kHidden];
+    }
+    __syncthreads();
+    // ---- loss: F_hat = y(upper) - y(lower); dL/dy = +-2 e / B ----
+    if (tid < kTrSamples) {
+        const int smp = s0 + tid;
+        float d = 0.0f;
+        if (smp < B) {
+            const float e = (y[tid] - y[kTrSamples + tid]) - target[smp];
+            d = 2.0f * e / (float)B;
+            if (loss_terms) loss_terms[smp] = (double)e * (double)e;
+        }
+        dy[tid] = d;
+        dy[kTrSamples + tid] = -d;
+    }
+    __syncthreads();
+    // ---- backward ----
+    // output layer: gW4[k] = sum_m dy silu(A3), gb4 = sum_m dy; D0 = dy W4 silu'(A3)
+    for (int k = tid; k < kHidden; k += kTrThreads) {
+        float g = 0.0f;
+        for (int m = 0; m < kTrRows; ++m) g += dy[m] * silu(A3[m * kLdH + k]);
+        out[OFF_W4 + k] = g;
+    }
+    if (tid == kHidden) {
+        float g = 0.0f;
+        for (int m = 0; m < kTrRows; ++m) g += dy[m];
+        out[OFF_B4] = g;
+    }
+    for (int i = tid; i < kTrRows * kHidden; i += kTrThreads) {
+        const int m = i / kHidden, n = i % kHidden;
+        D0[m * kLdH + n] = dy[m] * w4[n] * silu_grad(A3[m * kLdH + n]);
+    }
+    __syncthreads();
+    // layer 3 (H = silu(A2) still holds its input): gW3 = D0^T H, gb3 = colsum D0; D1 = (D0 W3) silu'(A2)
+    tr_gemm<kHidden, kHidden, kTrRows>([&](int n, int m) { return D0[m * kLdH + n]; },
+                                       [&](int m, int k) { return H[m * kLdH + k]; },
+                                       [&](int n, int k, float v) { out[OFF_W3 + n * kHidden + k] = v; }, warp, lane);
+    tr_gemm<kTrRows, kHidden, kHidden>([&](int m, int n) { return D0[m * kLdH + n]; },
+                                       [&](int n, int k) { return W3[n * kLdH + k]; },
+                                       [&](int m, int k, float v) { D1[m * kLdH + k] = v * silu_grad(A2[m * kLdH + k]); },
+                                       warp, lane);
+    for (int n = tid; n < kHidden; n += kTrThreads) {
+        float g = 0.0f;
+        for (int m = 0; m < kTrRows; ++m) g += D0[m * kLdH + n];
+        out[OFF_B3 + n] = g;
+    }
+    __syncthreads();
+    for (int i = tid; i < kTrRows * kHidden; i += kTrThreads) {
+        const int m = i / kHidden, n = i % kHidden;
+        H[m * kLdH + n] = silu(A1[m * kLdH + n]);
+    }
+    __syncthreads();
+    // layer 2: gW2 = D1^T silu(A1), gb2; D0 = (D1 W2) silu'(A1)
+    tr_gemm<kHidden, kHidden, kTrRows>([&](int n, int m) { return D1[m * kLdH + n]; },
+                                       [&](int m, int k) { return H[m * kLdH + k]; },
+                                       [&](int n, int k, float v) { out[OFF_W2 + n * kHidden + k] = v; }, warp, lane);
+    tr_gemm<kTrRows, kHidden, kHidden>([&](int m, int n) { return D1[m * kLdH + n]; },
+                                       [&](int n, int k) { return W2[n * kLdH + k]; },
+                                       [&](int m, int k, float v) { D0[m * kLdH + k] = v * silu_grad(A1[m * kLdH + k]); },
+                                       warp, lane);
+    for (int n = tid; n < kHidden; n += kTrThreads) {
+        float g = 0.0f;
+        for (int m = 0; m < kTrRows; ++m) g += D1[m * kLdH + n];
+        out[OFF_B2 + n] = g;
+    }
+    __syncthreads();
+    // layer 1: gW1 = D0^T X0 (inputs 0 .. 17), gb1; dX0 = D0 W1 (the embedding's 16 inputs) into H
+    tr_gemm<kHidden, kIn8, kTrRows>([&](int n, int m) { return D0[m * kLdH + n]; },
+                                    [&](int m, int k) { return X0[m * kLd1 + k]; },
+                                    [&](int n, int k, float v) {
+                                        if (k < kIn) out[OFF_W1 + n * kIn + k] = v;
+                                    },
+                                    warp, lane);
+    tr_gemm<kTrRows, kEmbed, kHidden>([&](int m, int n) { return D0[m * kLdH + n]; },
+                                      [&](int n, int k) { return W1[n * kLd1 + k]; },
+                                      [&](int m, int k, float v) { H[m * kLdH + k] = v; }, warp, lane);
+    for (int n = tid; n < kHidden; n += kTrThreads) {
+        float g = 0.0f;
+        for (int m = 0; m < kTrRows; ++m) g += D0[m * kLdH + n];
+        out[OFF_B1 + n] = g;
+    }
+    __syncthreads();
+    // embedding: gEmb[Z][k] = sum over the block's rows of element Z, in row order (zero for the others)
+    for (int i = tid; i < 103 * kEmbed; i += kTrThreads) {
         const int zz = i / kEmbed + 1, k = i % kEmbed;
-        float s = 0.0f;
-        for (int b = 0; b < B; ++b)
-            if (z[b] == zz) s += dX0[b * kIn + k];
-        demb[i] = s;
+        float g = 0.0f;
+        for (int m = 0; m < kTrRows; ++m)
+            if (zr[m] == zz) g += H[m * kLdH + k];
+        out[OFF_EMB + i] = g;
     }
 }
 
-__global__ void k_sg_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
-                          float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+// g = sum over the blocks' rows of `partial` in block order; with lr > 0 also the Adam step on p.
+__global__ void k_sg_reduce_adam(const float* __restrict__ partial, int blocks, float* __restrict__ grads,
+                                 float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, int n, float lr,
+                                 float b1, float b2, float eps, float c1, float c2) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float gi = g[i];
-        const float mi = b1 * m[i] + (1.0f - b1) * gi;
-        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-        m[i] = mi;
-        v[i] = vi;
-        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        float gi = 0.0f;
+        for (int b = 0; b < blocks; ++b) gi += partial[(size_t)b * n + i];
+        grads[i] = gi;
+        if (lr > 0.0f) {
+            const float mi = b1 * m[i] + (1.0f - b1) * gi;
+            const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+            m[i] = mi;
+            v[i] = vi;
+            p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        }
     }
 }
 
@@ -358,20 +555,17 @@ double infinite_profile(int z, double rho) {
 
 namespace {
 
-struct Batch {  // a doubled batch: rows b (upper edge) and B + b (lower edge)
-    DeviceBuffer z, feats, target, x0, a1, h1, a2, h2, a3, h3, y, dy, d3, d2, d1, dx0, loss;
+struct Batch {  // a doubled batch: rows b (upper edge) and B + b (lower edge); per-block gradient rows
+    DeviceBuffer z, feats, target, loss, partial;
     void ensure(int B) {
         const int R = 2 * B;
         z.ensure(R * sizeof(int));
         feats.ensure((size_t)R * 2 * sizeof(float));
         target.ensure(B * sizeof(float));
-        x0.ensure((size_t)R * kIn * sizeof(float));
-        for (DeviceBuffer* b : {&a1, &h1, &a2, &h2, &a3, &h3, &d3, &d2, &d1}) b->ensure((size_t)R * kHidden * sizeof(float));
-        y.ensure(R * sizeof(float));
-        dy.ensure(R * sizeof(float));
-        dx0.ensure((size_t)R * kIn * sizeof(float));
         loss.ensure(B * sizeof(double));
+        partial.ensure((size_t)train_blocks(B) * kSurrogateParams * sizeof(float));
     }
+    static int train_blocks(int B) { return (B + kTrSamples - 1) / kTrSamples; }
 };
 
 // Host rows of one doubled batch from samples [first, first + B).
@@ -387,45 +581,32 @@ void fill_rows(const std::vector<int>& z, const std::vector<double>& rho, const 
     }
 }
 
-// Forward and backward of one doubled batch already in b: gradients into G, returns the loss when asked.
-double forward_backward(Context& ctx, const float* P, float* G, Batch& b, int B, bool want_loss) {
-    cudaStream_t s = ctx.stream;
-    const int R = 2 * B;
-    const int bl = blocks_for((long long)R * kHidden);
-    k_sg_x0<<<blocks_for((long long)R * kIn), 256, 0, s>>>(b.z.as<int>(), b.feats.as<float>(), P + OFF_EMB, R,
-                                                           b.x0.as<float>());
-    k_sg_linear<<<bl, 256, 0, s>>>(b.x0.as<float>(), P + OFF_W1, P + OFF_B1, R, kIn, kHidden, b.a1.as<float>(),
-                                   b.h1.as<float>());
-    k_sg_linear<<<bl, 256, 0, s>>>(b.h1.as<float>(), P + OFF_W2, P + OFF_B2, R, kHidden, kHidden, b.a2.as<float>(),
-                                   b.h2.as<float>());
-    k_sg_linear<<<bl, 256, 0, s>>>(b.h2.as<float>(), P + OFF_W3, P + OFF_B3, R, kHidden, kHidden, b.a3.as<float>(),
-                                   b.h3.as<float>());
-    k_sg_linear<<<blocks_for(R), 256, 0, s>>>(b.h3.as<float>(), P + OFF_W4, P + OFF_B4, R, kHidden, 1, b.y.as<float>(),
-                                              nullptr);
-    k_sg_loss<<<blocks_for(B), 256, 0, s>>>(b.y.as<float>(), b.target.as<float>(), B, b.dy.as<float>(),
-                                            b.loss.as<double>());
-    k_sg_grad_w<<<blocks_for(kHidden + 1), 256, 0, s>>>(b.dy.as<float>(), b.h3.as<float>(), R, kHidden, 1, G + OFF_W4,
-                                                        G + OFF_B4);
-    k_sg_grad_x<<<bl, 256, 0, s>>>(b.dy.as<float>(), P + OFF_W4, b.a3.as<float>(), R, kHidden, 1, b.d3.as<float>());
-    k_sg_grad_w<<<blocks_for(kHidden * (kHidden + 1)), 256, 0, s>>>(b.d3.as<float>(), b.h2.as<float>(), R, kHidden,
-                                                                    kHidden, G + OFF_W3, G + OFF_B3);
-    k_sg_grad_x<<<bl, 256, 0, s>>>(b.d3.as<float>(), P + OFF_W3, b.a2.as<float>(), R, kHidden, kHidden,
-                                   b.d2.as<float>());
-    k_sg_grad_w<<<blocks_for(kHidden * (kHidden + 1)), 256, 0, s>>>(b.d2.as<float>(), b.h1.as<float>(), R, kHidden,
-                                                                    kHidden, G + OFF_W2, G + OFF_B2);
-    k_sg_grad_x<<<bl, 256, 0, s>>>(b.d2.as<float>(), P + OFF_W2, b.a1.as<float>(), R, kHidden, kHidden,
-                                   b.d1.as<float>());
-    k_sg_grad_w<<<blocks_for(kHidden * (kIn + 1)), 256, 0, s>>>(b.d1.as<float>(), b.x0.as<float>(), R, kIn, kHidden,
-                                                                G + OFF_W1, G + OFF_B1);
-    k_sg_grad_x<<<blocks_for((long long)R * kIn), 256, 0, s>>>(b.d1.as<float>(), P + OFF_W1, nullptr, R, kIn, kHidden,
-                                                               b.dx0.as<float>());
-    k_sg_grad_emb<<<blocks_for(103 * kEmbed), 256, 0, s>>>(b.dx0.as<float>(), b.z.as<int>(), R, G + OFF_EMB);
-    ctx.launches += 15;
+void set_train_smem() {
+    static bool set = false;
+    if (!set) {
+        SIMK_CUDA(cudaFuncSetAttribute(k_sg_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem));
+        set = true;
+    }
+}
+
+// Forward and backward of the doubled batch at (z, feats, target): the gradient into G (and, with lr > 0, the Adam step
+// on P with moments m, v); returns the loss when asked (then it synchronises).
+double forward_backward(Context& ctx, float* P, float* G, const int* z, const float* feats, const float* target, int B,
+                        Batch& b, bool want_loss, float lr = 0.0f, float* m = nullptr, float* v = nullptr,
+                        float c1 = 1.0f, float c2 = 1.0f) {
+    cudaStream_t st = ctx.stream;
+    set_train_smem();
+    const int blocks = Batch::train_blocks(B);
+    k_sg_train<<<blocks, kTrThreads, kTrSmem, st>>>(P, z, feats, target, B, b.partial.as<float>(),
+                                                    want_loss ? b.loss.as<double>() : nullptr);
+    k_sg_reduce_adam<<<(kSurrogateParams + 255) / 256, 256, 0, st>>>(b.partial.as<float>(), blocks, G, P, m, v,
+                                                                    kSurrogateParams, lr, 0.9f, 0.999f, 1e-8f, c1, c2);
+    ctx.launches += 2;
     SIMK_CUDA(cudaGetLastError());
     if (!want_loss) return 0.0;
     std::vector<double> terms(B);
-    SIMK_CUDA(cudaMemcpyAsync(terms.data(), b.loss.ptr, B * sizeof(double), cudaMemcpyDeviceToHost, s));
-    SIMK_CUDA(cudaStreamSynchronize(s));
+    SIMK_CUDA(cudaMemcpyAsync(terms.data(), b.loss.ptr, B * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SIMK_CUDA(cudaStreamSynchronize(st));
     double sum = 0.0;
     for (double t : terms) sum += t;
     return sum / B;
@@ -569,27 +750,19 @@ std::unique_ptr<SurrogateImpl> surrogate_train(Context& ctx, const std::vector<i
     SIMK_CUDA(cudaMemcpy(targets.ptr, all_F.data(), n * sizeof(float), cudaMemcpyHostToDevice));
     Batch b;
     b.ensure(batch);
-    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float b1 = 0.9f, b2 = 0.999f;
     double loss = 0.0;
     for (int step = 0; step < steps; ++step) {
         const long long k = step % nb;
-        SIMK_CUDA(cudaMemcpyAsync(b.z.ptr, rows_z.as<int>() + k * 2 * batch, 2 * batch * sizeof(int),
-                                  cudaMemcpyDeviceToDevice, ctx.stream));
-        SIMK_CUDA(cudaMemcpyAsync(b.feats.ptr, rows_f.as<float>() + k * 4 * batch, 4 * batch * sizeof(float),
-                                  cudaMemcpyDeviceToDevice, ctx.stream));
-        SIMK_CUDA(cudaMemcpyAsync(b.target.ptr, targets.as<float>() + k * batch, batch * sizeof(float),
-                                  cudaMemcpyDeviceToDevice, ctx.stream));
         const bool want = (step == steps - 1);
-        const double l = forward_backward(ctx, s->params.as<float>(), s->grads.as<float>(), b, batch, want);
-        if (want) loss = l;
         // cosine decay from lr to lr / 20
         const double lr_t = lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(M_PI * step / (double)steps)));
         const float c1 = 1.0f - std::pow(b1, (float)(step + 1)), c2 = 1.0f - std::pow(b2, (float)(step + 1));
-        k_sg_adam<<<blocks_for(kSurrogateParams), 256, 0, ctx.stream>>>(s->params.as<float>(), s->grads.as<float>(),
-                                                                         s->m.as<float>(), s->v.as<float>(),
-                                                                         kSurrogateParams, (float)lr_t, b1, b2, eps,
-                                                                         c1, c2);
-        ++ctx.launches;
+        const double l = forward_backward(ctx, s->params.as<float>(), s->grads.as<float>(),
+                                          rows_z.as<int>() + k * 2 * batch, rows_f.as<float>() + k * 4 * batch,
+                                          targets.as<float>() + k * batch, batch, b, want, (float)lr_t,
+                                          s->m.as<float>(), s->v.as<float>(), c1, c2);
+        if (want) loss = l;
     }
     SIMK_CUDA(cudaGetLastError());
     s->train_loss = loss;
@@ -666,7 +839,8 @@ double surrogate_gradients(Context& ctx, SurrogateImpl& s, const std::vector<int
     SIMK_CUDA(cudaMemcpy(b.z.ptr, rz.data(), rz.size() * sizeof(int), cudaMemcpyHostToDevice));
     SIMK_CUDA(cudaMemcpy(b.feats.ptr, rf.data(), rf.size() * sizeof(float), cudaMemcpyHostToDevice));
     SIMK_CUDA(cudaMemcpy(b.target.ptr, y.data(), B * sizeof(float), cudaMemcpyHostToDevice));
-    const double loss = forward_backward(ctx, s.params.as<float>(), s.grads.as<float>(), b, B, true);
+    const double loss = forward_backward(ctx, s.params.as<float>(), s.grads.as<float>(), b.z.as<int>(),
+                                         b.feats.as<float>(), b.target.as<float>(), B, b, true);
     SIMK_CUDA(cudaMemcpy(grads_host, s.grads.ptr, kSurrogateParams * sizeof(float), cudaMemcpyDeviceToHost));
     return loss;
 }

@@ -250,21 +250,26 @@ __device__ __forceinline__ bool tc5_fft(const float2* __restrict__ src, const fl
     float d[16];
     if (ok) tmem_ld16(d_col, d);
     // ---- stage B: the outputs of stage A, twiddled for stage B and split, scattered into the A rows they feed ----
+    // Output s = 8 h + i of stage A sits at (j - k) 16 + k + s NSA (k = j mod NSA) and is input rb of stage-B vector jb:
+    // for R = 2, jb = k + 2 s and rb = j / 2; for R = 1, jb = s and rb = j. So along i the stage-B vector steps by
+    // NSA (its A row by NSA LINES for column tiles, NSA for row tiles), the input rb is fixed, and the twiddle
+    // W_N^{jb rb} steps by NSA rb: one base address and constant strides per thread, all in one 128-vector block.
     {
         const int k = j % NSA;
+        const int rb = (R == 2) ? (j >> 1) : j;
+        const int vb0 = row_of(R == 2 ? k + 16 * h : 8 * h);
+        constexpr int kRowStep = NSA * (COLS ? LINES : 1);
+        uint8_t* p0 = a_blk + (size_t)(vb0 >> 7) * 3 * kTc5Plane + (size_t)(vb0 & 127) * 16 +
+                      (size_t)(rb >> 2) * kTc5Lbo + (size_t)(rb & 3) * 4;
+        const float2* w0 = tw + (R == 2 ? (k + 16 * h) : 8 * h) * rb;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const int s = 8 * h + i;
-            const int pos = (j - k) * 16 + k + s * NSA;  // stage A's output position
-            const int jb = pos % NV, rb = pos / NV;     // the vector of stage B it feeds, and which input
             float2 x = make_float2(d[2 * i], d[2 * i + 1]);
-            const float2 w = __ldg(tw + (jb % NSB) * rb * (N / (16 * NSB)));
+            const float2 w = __ldg(w0 + i * NSA * rb);
             x = (DIR < 0) ? cmul(x, w) : cmulc(x, w);
             uint32_t hh, ll, l2;
             tc5_split3(x, hh, ll, l2);
-            const int vb = row_of(jb);
-            uint8_t* p = a_blk + (size_t)(vb >> 7) * 3 * kTc5Plane + (size_t)(vb & 127) * 16 +
-                         (size_t)(rb >> 2) * kTc5Lbo + (size_t)(rb & 3) * 4;
+            uint8_t* p = p0 + i * kRowStep * 16;
             *reinterpret_cast<uint32_t*>(p) = hh;
             *reinterpret_cast<uint32_t*>(p + kTc5Plane) = ll;
             *reinterpret_cast<uint32_t*>(p + 2 * kTc5Plane) = l2;
