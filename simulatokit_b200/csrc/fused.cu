@@ -252,9 +252,18 @@ __device__ __forceinline__ void tw_load(TwRegs<N>& tr, unsigned t, const float2*
     }
 }
 
-template <int N, int F, int DIR, int STRIDE>
+// The barrier of one line's exchange: the whole block (LT = 0), or only the LT threads of the line (whole warps, from
+// warp 32 (id - 1) / ... on): one warp needs no barrier beyond __syncwarp; more use the named barrier `id` (1-15).
+template <int LT>
+__device__ __forceinline__ void line_sync(int id) {
+    if constexpr (LT == 0) __syncthreads();
+    else if constexpr (LT == 32) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(LT) : "memory");
+}
+
+template <int N, int F, int DIR, int STRIDE, int LT = 0>
 __device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const TwRegs<N>& tr,
-                                            const SmemCT<STRIDE>& sm) {
+                                            const SmemCT<STRIDE>& sm, int bar_id = 0) {
     using P = Pow2<N>;
     if constexpr (F < P::NP) {
         constexpr int R = P::radix(F), NS = P::ns(F), Q = 8 / R;
@@ -286,12 +295,12 @@ __device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const Tw
             }
         }
         if constexpr (SC) {
-            __syncthreads();
+            line_sync<LT>(bar_id);
 #pragma unroll
             for (int i = 0; i < 8; ++i) v[i] = sm.at((int)t + P::T * i);
-            __syncthreads();
+            line_sync<LT>(bar_id);
         }
-        ct_fft_from<N, F + 1, DIR, STRIDE>(v, t, tr, sm);
+        ct_fft_from<N, F + 1, DIR, STRIDE, LT>(v, t, tr, sm, bar_id);
     }
 }
 
@@ -724,12 +733,15 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
         if (abort_flag) break;
         float2* row = psi + (size_t)(tile * RB + rr) * N;
         if constexpr (ENG == 0) {
+            // a row's exchanges stay in its own part of the stage: only the row's threads synchronise
+            constexpr int LT = (RB > 1 && T % 32 == 0 && RB < 16) ? T : 0;
+            const int bar = 1 + rr;
             float2 v[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) v[i] = buf[rr * N + t + T * i];
-            __syncthreads();
+            line_sync<LT>(bar);
             SmemCT<0> sm{buf + rr * N};
-            if (inv) ct_fft_from<N, 0, +1>(v, t, eng, sm);
+            if (inv) ct_fft_from<N, 0, +1, 0, LT>(v, t, eng, sm, bar);
             if (with_t) {
 #pragma unroll
                 for (int i = 0; i < 8; ++i) v[i] = cmul(v[i], tbuf[rr * N + t + T * i]) * scale;
@@ -737,7 +749,7 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
 #pragma unroll
                 for (int i = 0; i < 8; ++i) v[i] = v[i] * scale;
             }
-            if (fwd) ct_fft_from<N, 0, -1>(v, t, eng, sm);
+            if (fwd) ct_fft_from<N, 0, -1, 0, LT>(v, t, eng, sm, bar);
             // back into the stage rows (every exchange read is behind a barrier); thread 0 stores them after the
             // barrier below
 #pragma unroll
