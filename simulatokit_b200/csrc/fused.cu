@@ -1674,6 +1674,33 @@ void incident_wave(Context& ctx, const JobSpec& j, float2* psi) {
     SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the temporaries above are freed on return
 }
 
+// One grid shape's jobs in a fused job-table run: their waves, intensities, per-step tables and stream.
+struct GroupRun {
+    std::vector<int> ids;     // job indices, longest first
+    std::vector<int> slices;  // their slice counts
+    int G = 0, S = 0, nx = 0, ny = 0, first_in_order = 0, pblocks = 0;
+    long long N = 0;
+    DeviceBuffer waves, inten, pstack, dt, dp;
+    cudaStream_t stream = nullptr;
+};
+
+// The groups' streams and their start event: on exit (also by an exception) the context's stream is restored, every
+// stream drained and destroyed.
+struct StreamsScope {
+    Context& c;
+    cudaStream_t home;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    ~StreamsScope() {
+        c.stream = home;
+        for (auto st : streams) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        for (auto e : events) cudaEventDestroy(e);
+    }
+};
+
 // Resets the context's wave table when a job run ends, also by an exception.
 struct WaveTableScope {
     Context& c;
@@ -1718,6 +1745,8 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
     std::vector<int> order;
     SIMK_CUDA(cudaEventRecord(start, ctx.stream));
     WaveTableScope scope{ctx};
+    std::vector<GroupRun> runs;  // the fused form's groups, set up first, then advanced side by side
+    runs.reserve(groups.size());
     try {
         for (auto& kv : groups) {
             const std::vector<int>& ids = kv.second;
@@ -1753,6 +1782,16 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
                 continue;
             }
             // per step: each wave's transmission slice and propagator block
+            GroupRun& gr = runs.emplace_back();
+            gr.ids = ids;
+            gr.G = G;
+            gr.S = S;
+            gr.N = N;
+            gr.nx = nx;
+            gr.ny = ny;
+            gr.first_in_order = first_in_order;
+            gr.waves = std::move(waves);
+            gr.inten = std::move(inten);
             std::vector<const float2*> tptr((size_t)S * G, nullptr);
             std::vector<int> prow((size_t)S * G, 0);
             std::vector<const float2*> pblocks;
@@ -1771,55 +1810,88 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
                     prow[(size_t)s * G + w] = it->second;
                 }
             }
-            DeviceBuffer pstack(pblocks.size() * N * sizeof(float2)), dt(tptr.size() * sizeof(float2*)),
-                dp(prow.size() * sizeof(int));
+            gr.pblocks = (int)pblocks.size();
+            gr.pstack.alloc(pblocks.size() * N * sizeof(float2));
+            gr.dt.alloc(tptr.size() * sizeof(float2*));
+            gr.dp.alloc(prow.size() * sizeof(int));
             for (size_t b = 0; b < pblocks.size(); ++b)
-                SIMK_CUDA(cudaMemcpyAsync(pstack.as<float2>() + (long long)b * N, pblocks[b], N * sizeof(float2),
+                SIMK_CUDA(cudaMemcpyAsync(gr.pstack.as<float2>() + (long long)b * N, pblocks[b], N * sizeof(float2),
                                           cudaMemcpyDeviceToDevice, ctx.stream));
-            SIMK_CUDA(cudaMemcpyAsync(dt.ptr, tptr.data(), tptr.size() * sizeof(float2*), cudaMemcpyHostToDevice,
+            SIMK_CUDA(cudaMemcpyAsync(gr.dt.ptr, tptr.data(), tptr.size() * sizeof(float2*), cudaMemcpyHostToDevice,
                                       ctx.stream));
-            SIMK_CUDA(cudaMemcpyAsync(dp.ptr, prow.data(), prow.size() * sizeof(int), cudaMemcpyHostToDevice,
+            SIMK_CUDA(cudaMemcpyAsync(gr.dp.ptr, prow.data(), prow.size() * sizeof(int), cudaMemcpyHostToDevice,
                                       ctx.stream));
-            const RegPlan prw = reg_plan(ctx, ny);
-            const RegPlan pcl = reg_plan(ctx, nx);
-            auto active = [&](int s) {  // jobs with more than s slices: a prefix
-                int a = 0;
-                while (a < G && jobs[ids[a]].pot->n_slices() > s) ++a;
-                return a;
-            };
-            for (int s = 0; s < S; ++s) {
-                const int A = active(s);
-                ctx.wave_t = dt.as<const float2*>() + (size_t)s * G;
-                ctx.wave_p = dp.as<int>() + (size_t)s * G;
-                ctx.wave_p_blocks = (int)pblocks.size();
-                launch_rows(ctx, prw, psi, nullptr, nx, (long long)A * nx, s > 0 ? 1 : 0, 1, 1.0f);
-                ColArgs a{};
-                a.psi = psi;
-                a.P = pstack.as<float2>();
-                a.ny = ny;
-                a.mode = 0;
-                a.pscale = 1.0f / (float)N;
-                launch_cols(ctx, pcl, a, A);
-                ctx.wave_t = nullptr;
-                ctx.wave_p = nullptr;
-                ctx.wave_p_blocks = 0;
-                const int A1 = active(s + 1);
-                if (A1 == A) continue;
-                // jobs A1 .. A-1 have ended: complete their row inverse transform, intensities out
-                finish_rows(ctx, g0, psi + (long long)A1 * N, A - A1);
-                k_intensity<<<grid_for((long long)(A - A1) * N), 256, 0, ctx.stream>>>(
-                    psi + (long long)A1 * N, (long long)(A - A1) * N, inten.as<double>() + (long long)A1 * N);
-                ++ctx.launches;
-                cudaEvent_t e;
-                SIMK_CUDA(cudaEventCreate(&e));
-                SIMK_CUDA(cudaEventRecord(e, ctx.stream));
-                events.push_back(e);
-                event_jobs.push_back({first_in_order + A1, first_in_order + A});
+            gr.slices.resize(G);
+            for (int w = 0; w < G; ++w) gr.slices[w] = jobs[ids[w]].pot->n_slices();
+            SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the host tables above are freed on return
+        }
+        // The groups' slice steps, each group on its own stream so that the shapes run side by side (the launches of a
+        // step depend only on the same group's previous step): step s of every group still running, in turn.
+        if (!runs.empty()) {
+            cudaStream_t home = ctx.stream;
+            StreamsScope streams{ctx, home};
+            cudaEvent_t go;
+            SIMK_CUDA(cudaEventCreateWithFlags(&go, cudaEventDisableTiming));
+            streams.events.push_back(go);
+            SIMK_CUDA(cudaEventRecord(go, home));
+            for (auto& gr : runs) {
+                cudaStream_t st;
+                SIMK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                streams.streams.push_back(st);
+                SIMK_CUDA(cudaStreamWaitEvent(st, go, 0));
+                gr.stream = st;
             }
-            for (int w = 0; w < G; ++w)
-                SIMK_CUDA(cudaMemcpyAsync(jobs[ids[w]].intensity, inten.as<double>() + (long long)w * N,
-                                          N * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
-            SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the group's buffers are freed here
+            int max_s = 0;
+            for (auto& gr : runs) max_s = std::max(max_s, gr.S);
+            for (int s = 0; s < max_s; ++s) {
+                for (auto& gr : runs) {
+                    if (s >= gr.S) continue;
+                    ctx.stream = gr.stream;
+                    const int G = gr.G;
+                    auto active = [&](int ss) {  // jobs with more than ss slices: a prefix
+                        int a = 0;
+                        while (a < G && gr.slices[a] > ss) ++a;
+                        return a;
+                    };
+                    const int A = active(s);
+                    const RegPlan prw = reg_plan(ctx, gr.ny);
+                    const RegPlan pcl = reg_plan(ctx, gr.nx);
+                    float2* psi = gr.waves.as<float2>();
+                    ctx.wave_t = gr.dt.as<const float2*>() + (size_t)s * G;
+                    ctx.wave_p = gr.dp.as<int>() + (size_t)s * G;
+                    ctx.wave_p_blocks = gr.pblocks;
+                    launch_rows(ctx, prw, psi, nullptr, gr.nx, (long long)A * gr.nx, s > 0 ? 1 : 0, 1, 1.0f);
+                    ColArgs a{};
+                    a.psi = psi;
+                    a.P = gr.pstack.as<float2>();
+                    a.ny = gr.ny;
+                    a.mode = 0;
+                    a.pscale = 1.0f / (float)gr.N;
+                    launch_cols(ctx, pcl, a, A);
+                    ctx.wave_t = nullptr;
+                    ctx.wave_p = nullptr;
+                    ctx.wave_p_blocks = 0;
+                    const int A1 = active(s + 1);
+                    if (A1 == A) continue;
+                    // jobs A1 .. A-1 have ended: complete their row inverse transform, intensities out
+                    const GridGeom g1{gr.nx, gr.ny, 0.0, 0.0};
+                    finish_rows(ctx, g1, psi + (long long)A1 * gr.N, A - A1);
+                    k_intensity<<<grid_for((long long)(A - A1) * gr.N), 256, 0, ctx.stream>>>(
+                        psi + (long long)A1 * gr.N, (long long)(A - A1) * gr.N, gr.inten.as<double>() + (long long)A1 * gr.N);
+                    ++ctx.launches;
+                    cudaEvent_t e;
+                    SIMK_CUDA(cudaEventCreate(&e));
+                    SIMK_CUDA(cudaEventRecord(e, ctx.stream));
+                    events.push_back(e);
+                    event_jobs.push_back({gr.first_in_order + A1, gr.first_in_order + A});
+                }
+            }
+            for (auto& gr : runs) {
+                for (int w = 0; w < gr.G; ++w)
+                    SIMK_CUDA(cudaMemcpyAsync(jobs[gr.ids[w]].intensity, gr.inten.as<double>() + (long long)w * gr.N,
+                                              gr.N * sizeof(double), cudaMemcpyDeviceToHost, gr.stream));
+            }
+            for (auto& gr : runs) SIMK_CUDA(cudaStreamSynchronize(gr.stream));
         }
         SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
         check_device_error(ctx);
