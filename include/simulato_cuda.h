@@ -54,8 +54,9 @@ extern "C" {
 #define SIMK_OPT_TUNED_TMA 10
 #define SIMK_OPT_TUNED_BATCH 11
 /* The bf16x3 form's radix-16 DFT stages on the fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
- * memory) for grid sides 256 and 512, with the data split in three BF16 terms; 0 = the warp-level mma.sync stages
- * (data in two terms) everywhere. Default 1. */
+ * memory) for grid sides 256 and 512, with the data split in three BF16 terms: 1 (default) = twelve products of
+ * N = 32 per block of 128 vectors; 2 = the same sums as six products of N = 96, 64 and 32 (the B terms stacked) whose
+ * three accumulator blocks the threads add; 0 = the warp-level mma.sync stages (data in two terms) everywhere. */
 #define SIMK_OPT_TCGEN05 12
 /* Sum the annular, centre-of-mass and segmented detectors inside the fused form's last column pass (TMA passes), so
  * the k-space waves are neither written nor read back unless a pixelated or binned detector wants them; 0 = detect

@@ -153,7 +153,10 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                 break;
             case SIMK_OPT_TMA: c.tma = value ? 1 : 0; break;
             case SIMK_OPT_AUTOTUNE: c.autotune = value ? 1 : 0; break;
-            case SIMK_OPT_TCGEN05: c.tcgen05 = value ? 1 : 0; break;
+            case SIMK_OPT_TCGEN05:
+                SIMK_REQUIRE(value >= 0 && value <= 2, "tcgen05 option must be 0, 1 or 2");
+                c.tcgen05 = (int)value;
+                break;
             case SIMK_OPT_EPILOGUE_DETECT: c.epilogue_detect = value ? 1 : 0; break;
             case SIMK_OPT_POISSON_STREAM:
                 SIMK_REQUIRE(value == 0 || value == 1, "Poisson stream must be 0 (per value) or 1 (reference order)");

@@ -464,8 +464,9 @@ constexpr int tc5_blocks(int n, int lines) { return n * lines / 2048; }
 
 // Engine 3's set-up, by every thread of the block: tensor memory (warp 0), the B matrices, the MMA barrier.
 template <int MB>
-__device__ __forceinline__ Tc5 tc5_setup(uint8_t* area, uint32_t* tmem_slot, uint64_t* mma_bar, int tid, int nthreads) {
-    if (tid < 32) tmem_alloc(tmem_slot, tc5_tmem_cols(MB));
+__device__ __forceinline__ Tc5 tc5_setup(uint8_t* area, uint32_t* tmem_slot, uint64_t* mma_bar, int tid, int nthreads,
+                                         int stack) {
+    if (tid < 32) tmem_alloc(tmem_slot, tc5_tmem_cols(MB, stack != 0));
     tc5_build_b(area + (size_t)MB * 3 * kTc5Plane, tid, nthreads);
     if (tid == 0) {
         mbar_init(mma_bar, 1);
@@ -482,6 +483,7 @@ __device__ __forceinline__ Tc5 tc5_setup(uint8_t* area, uint32_t* tmem_slot, uin
     c.tmem = *tmem_slot;
     c.bar = mma_bar;
     c.phase = 0;
+    c.stack = stack;
     return c;
 }
 
@@ -495,7 +497,7 @@ __device__ __forceinline__ void tc5_release(const Tc5& c, int tid, bool aborted)
     __syncthreads();
     if (tid < 32) {
         tc_fence_after();
-        tmem_dealloc(c.tmem, tc5_tmem_cols(MB));
+        tmem_dealloc(c.tmem, tc5_tmem_cols(MB, c.stack != 0));
     }
 }
 
@@ -515,7 +517,8 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
                                                                const __grid_constant__ CUtensorMap pmap,
                                                                float2* __restrict__ psi, float pscale, int ny,
                                                                int count, const float2* __restrict__ tw, int* err,
-                                                               const int* __restrict__ p_row, const DetectArgs det) {
+                                                               const int* __restrict__ p_row, const DetectArgs det,
+                                                               int tc5_stack) {
     extern __shared__ __align__(128) unsigned char smem_tma[];
     constexpr int T = N / 8;
     constexpr int BOXH = tma_box_rows(N);
@@ -544,7 +547,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     else if constexpr (ENG == 3)
         eng = tc5_setup<tc5_blocks(N, TC)>(smem_tma + 4 * (size_t)TILE * sizeof(float2), &tmem_slot, &mma_bar, tid,
-                                           TC * T);
+                                           TC * T, tc5_stack);
     auto issue = [&](unsigned tile, int s) {
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
@@ -676,7 +679,8 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
                                                                const float2* __restrict__ tmul,
                                                                const float2* __restrict__ tw, int nx, int nrows,
                                                                int inv, int fwd, float scale, int* err,
-                                                               const float2* const* __restrict__ t_of_wave) {
+                                                               const float2* const* __restrict__ t_of_wave,
+                                                               int tc5_stack) {
     extern __shared__ __align__(128) unsigned char smem_rtma[];
     constexpr int T = N / 8;
     constexpr int TILE = N * RB;
@@ -703,7 +707,7 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     else if constexpr (ENG == 3)
         eng = tc5_setup<tc5_blocks(N, RB)>(smem_rtma + 4 * (size_t)TILE * sizeof(float2), &tmem_slot, &mma_bar, tid,
-                                           RB * T);
+                                           RB * T, tc5_stack);
     constexpr bool kStoreFromStage = (ENG == 0 || ENG == 3);  // the finished rows go back by a bulk store
     auto issue = [&](int tile, int s) {
         float2* dst = stages + s * 2 * TILE;
@@ -995,8 +999,8 @@ constexpr size_t tma_pass_smem(int n, int lines, int eng) {
 }
 
 // Blocks per SM of a persistent pass: the occupancy, and for the tcgen05 engine at most what tensor memory holds.
-inline int pass_blocks_per_sm(int occupancy, int eng, int mb) {
-    if (eng == 3) occupancy = std::min(occupancy, 512 / (int)tc5_tmem_cols(mb));
+inline int pass_blocks_per_sm(int occupancy, int eng, int mb, bool stack) {
+    if (eng == 3) occupancy = std::min(occupancy, 512 / (int)tc5_tmem_cols(mb, stack));
     return occupancy;
 }
 
@@ -1011,18 +1015,19 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
     const size_t smem = tma_pass_smem(N, RB, ENG);
     auto kern = fused_rows_tma<N, RB, ENG>;
-    static int blocks_per_sm = -1;
-    if (blocks_per_sm < 0) {
+    static int occupancy = -1;
+    if (occupancy < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, RB * T, smem));
-        blocks_per_sm = pass_blocks_per_sm(blocks_per_sm, ENG, ENG == 3 ? tc5_blocks(N, RB) : 0);
+        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, RB * T, smem));
     }
+    const int stack = ctx.tcgen05 == 2 ? 1 : 0;
+    const int blocks_per_sm = pass_blocks_per_sm(occupancy, ENG, ENG == 3 ? tc5_blocks(N, RB) : 0, stack != 0);
     if (blocks_per_sm <= 0) return false;
     ensure_err_flag(ctx);
     const long long ntiles = nrows / RB;
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(T, RB), smem, ctx.stream>>>(psi, tmul, p.tw, nx, (int)nrows, inv, fwd, scale,
-                                                  ctx.err_flag.as<int>(), ctx.wave_t);
+                                                  ctx.err_flag.as<int>(), ctx.wave_t, stack);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
@@ -1038,12 +1043,13 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     } else {
     const size_t smem = tma_pass_smem(N, TC, ENG);
     auto kern = fused_cols_tma<N, TC, MODE, ENG>;
-    static int blocks_per_sm = -1;
-    if (blocks_per_sm < 0) {
+    static int occupancy = -1;
+    if (occupancy < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, TC * T, smem));
-        blocks_per_sm = pass_blocks_per_sm(blocks_per_sm, ENG, ENG == 3 ? tc5_blocks(N, TC) : 0);
+        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, TC * T, smem));
     }
+    const int stack = ctx.tcgen05 == 2 ? 1 : 0;
+    const int blocks_per_sm = pass_blocks_per_sm(occupancy, ENG, ENG == 3 ? tc5_blocks(N, TC) : 0, stack != 0);
     if (blocks_per_sm <= 0) return false;
     ensure_err_flag(ctx);
     const CUtensorMap map = encode_tensor_map_2d(a.psi, 2ULL * a.ny, (unsigned long long)count * N, 2 * TC, BOXH);
@@ -1064,7 +1070,7 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     }
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(TC, T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
-                                                  ctx.err_flag.as<int>(), a.p_row, det);
+                                                  ctx.err_flag.as<int>(), a.p_row, det, stack);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;

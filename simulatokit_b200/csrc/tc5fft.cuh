@@ -19,8 +19,13 @@
 // Shared memory of a block: per block of 128 vectors three A planes (hi, lo, lo2), each K-major without swizzle: the
 // 16-byte chunk c (K = 8c .. 8c + 7, i.e. inputs r = 4c .. 4c + 3) of row v at c * kTc5Lbo + v * 16 (core matrices
 // of 8 rows x 16 bytes, 128 bytes apart along M: SBO = 128; chunks kTc5Lbo apart along K: LBO). kTc5Lbo = 2080 rather
-// than 2048 spreads the 4-byte scatter of the second stage over all 32 banks. Then the six B matrices
-// ([inverse][term]), each 32 rows x 4 chunks with LBO 512, SBO 128.
+// than 2048 spreads the 4-byte scatter of the second stage over all 32 banks. Then the B operand of each direction:
+// the three terms' 32 rows stacked (rows 0-31 B_hi, 32-63 B_lo, 64-95 B_lo2), 4 chunks with LBO 1536, SBO 128, so
+// that one descriptor covers B_hi (N = 32), B_hi and B_lo (N = 64) or all three (N = 96).
+//
+// Products. Either twelve instructions of N = 32, each A term times each B term it pairs with accumulating into one
+// 32-column D (the default), or six of N = 96, 64, 32 (`stack`): A_hi times [B_hi B_lo B_lo2], A_lo times
+// [B_hi B_lo], A_lo2 times B_hi into three 32-column blocks of D, which the threads add as they read them.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -33,15 +38,21 @@ namespace simk {
 
 constexpr uint32_t kTc5Lbo = 2080;                        // bytes between K chunks of an A plane
 constexpr uint32_t kTc5Plane = 3 * kTc5Lbo + 2048;        // one A plane (4 chunks of 128 rows x 16 bytes)
-constexpr uint32_t kTc5BLbo = 512;                        // bytes between K chunks of a B matrix
-constexpr uint32_t kTc5BBytes = 4 * kTc5BLbo;             // one B matrix (32 rows x 64 bytes)
-// Shared-memory bytes of the engine for MB blocks of 128 vectors: the A planes, then the six B matrices.
-constexpr uint32_t tc5_smem_bytes(int mb) { return (uint32_t)mb * 3u * kTc5Plane + 6u * kTc5BBytes; }
-// Tensor-memory columns: 32 float32 accumulator columns per block of 128 vectors (a power of two, at least 32).
-constexpr uint32_t tc5_tmem_cols(int mb) { return mb <= 1 ? 32u : (mb <= 2 ? 64u : 128u); }
+constexpr uint32_t kTc5BLbo = 96 * 16;                    // bytes between K chunks of a direction's B (96 rows)
+constexpr uint32_t kTc5BBytes = 4 * kTc5BLbo;             // one direction's B (3 terms x 32 rows x 64 bytes)
+// Shared-memory bytes of the engine for MB blocks of 128 vectors: the A planes, then both directions' B.
+constexpr uint32_t tc5_smem_bytes(int mb) { return (uint32_t)mb * 3u * kTc5Plane + 2u * kTc5BBytes; }
+// Tensor-memory columns per block of 128 vectors: 32 float32 accumulator columns, or 128 (96 used) with the stacked
+// products; a power of two, at least 32.
+__host__ __device__ constexpr uint32_t tc5_tmem_cols(int mb, bool stack = false) {
+    return stack ? (uint32_t)mb * 128u : (mb <= 1 ? 32u : (mb <= 2 ? 64u : 128u));
+}
+__host__ __device__ constexpr uint32_t tc5_block_cols(bool stack) { return stack ? 128u : 32u; }
 // Instruction descriptor of kind::f16: D float32 (bits 4-5 = 1), A and B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major,
-// N >> 3 in bits 17-22, M >> 4 in bits 24-28.
-constexpr uint32_t kTc5Idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// N >> 3 in bits 17-22, M >> 4 in bits 24-28 (M = 128; N = 32, 64 or 96, multiples of 16 as M = 128 requires).
+__host__ __device__ constexpr uint32_t tc5_idesc(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
 
 // ---- tcgen05 instructions ---------------------------------------------------------------------------------------------
 // One warp allocates `ncols` tensor-memory columns and writes their address to *slot (shared memory).
@@ -64,14 +75,16 @@ __device__ __forceinline__ uint64_t tc5_desc(uint32_t saddr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// D (tensor memory) = A B^T (+ D when accumulate): M = 128, N = 32, K = 16, issued by the calling thread alone.
-__device__ __forceinline__ void tc5_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// D (tensor memory) = A B^T (+ D when accumulate): M = 128, K = 16, N from the instruction descriptor, issued by the
+// calling thread alone.
+__device__ __forceinline__ void tc5_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
     const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(kTc5Idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
         "r"(mask3)
         : "memory");
 }
@@ -123,6 +136,7 @@ struct Tc5 {
     uint32_t tmem;     // tensor-memory address of the accumulators (lane 0)
     uint64_t* bar;     // the MMA completion barrier
     uint32_t phase;    // its next parity
+    int stack;         // six stacked products (N = 96, 64, 32) instead of twelve of N = 32
 };
 
 // The six B matrices (forward, inverse) x (hi, lo, lo2) into shared memory at `b` by all `nthreads` threads, from
@@ -139,36 +153,67 @@ __device__ __forceinline__ void tc5_build_b(uint8_t* b, int tid, int nthreads) {
         const double r1 = val - (double)__bfloat162float(h);
         const __nv_bfloat16 l = __double2bfloat16(r1);
         const __nv_bfloat16 l2 = __double2bfloat16(r1 - (double)__bfloat162float(l));
+        // term t's row n sits at row 32 t + n of the direction's stacked matrix
         const uint32_t off = (uint32_t)(k >> 3) * kTc5BLbo + (uint32_t)n * 16u + (uint32_t)(k & 7) * 2u;
-        *reinterpret_cast<__nv_bfloat16*>(b + (inv * 3 + 0) * kTc5BBytes + off) = h;
-        *reinterpret_cast<__nv_bfloat16*>(b + (inv * 3 + 1) * kTc5BBytes + off) = l;
-        *reinterpret_cast<__nv_bfloat16*>(b + (inv * 3 + 2) * kTc5BBytes + off) = l2;
+        uint8_t* bd = b + inv * kTc5BBytes + off;
+        *reinterpret_cast<__nv_bfloat16*>(bd) = h;
+        *reinterpret_cast<__nv_bfloat16*>(bd + 32 * 16) = l;
+        *reinterpret_cast<__nv_bfloat16*>(bd + 64 * 16) = l2;
     }
 }
 
-// Thread 0: the six products of every block of 128 vectors, then a commit to the barrier.
+// Thread 0: the products of every block of 128 vectors, then a commit to the barrier.
 template <int MB, int DIR>
 __device__ __forceinline__ void tc5_issue(const Tc5& c) {
     tc_fence_after();
     constexpr int inv = DIR > 0 ? 1 : 0;
-    // (A plane, B term): hi x lo2, hi x lo, lo x lo, lo2 x hi, lo x hi, hi x hi
-    constexpr int pa[6] = {0, 0, 1, 2, 1, 0};
-    constexpr int tb[6] = {2, 1, 1, 0, 0, 0};
+    const uint32_t bbase = c.b_base + (uint32_t)inv * kTc5BBytes;
+    const uint32_t bcols = tc5_block_cols(c.stack != 0);
 #pragma unroll
     for (int mb = 0; mb < MB; ++mb) {
+        const uint32_t d = c.tmem + (uint32_t)mb * bcols;
+        if (c.stack) {
+            // A_hi x [B_hi B_lo B_lo2] (N = 96, initialises all three blocks), A_lo x [B_hi B_lo], A_lo2 x B_hi
 #pragma unroll
-        for (int t = 0; t < 6; ++t) {
+            for (int pa = 0; pa < 3; ++pa) {
 #pragma unroll
-            for (int kk = 0; kk < 2; ++kk) {
-                const uint64_t ad = tc5_desc(c.a_base + (uint32_t)(mb * 3 + pa[t]) * kTc5Plane + 2u * kk * kTc5Lbo,
-                                             kTc5Lbo, 128);
-                const uint64_t bd = tc5_desc(c.b_base + (uint32_t)(inv * 3 + tb[t]) * kTc5BBytes + 2u * kk * kTc5BLbo,
-                                             kTc5BLbo, 128);
-                tc5_mma(c.tmem + (uint32_t)mb * 32u, ad, bd, (t | kk) != 0 ? 1u : 0u);
+                for (int kk = 0; kk < 2; ++kk) {
+                    const uint64_t ad = tc5_desc(c.a_base + (uint32_t)(mb * 3 + pa) * kTc5Plane + 2u * kk * kTc5Lbo,
+                                                 kTc5Lbo, 128);
+                    const uint64_t bd = tc5_desc(bbase + 2u * kk * kTc5BLbo, kTc5BLbo, 128);
+                    tc5_mma(d, ad, bd, tc5_idesc(96u - 32u * (uint32_t)pa), (pa | kk) != 0 ? 1u : 0u);
+                }
+            }
+        } else {
+            // (A plane, B term): hi x lo2, hi x lo, lo x lo, lo2 x hi, lo x hi, hi x hi into one 32-column D
+            constexpr int pa[6] = {0, 0, 1, 2, 1, 0};
+            constexpr int tb[6] = {2, 1, 1, 0, 0, 0};
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    const uint64_t ad = tc5_desc(c.a_base + (uint32_t)(mb * 3 + pa[t]) * kTc5Plane + 2u * kk * kTc5Lbo,
+                                                 kTc5Lbo, 128);
+                    const uint64_t bd = tc5_desc(bbase + (uint32_t)tb[t] * 32u * 16u + 2u * kk * kTc5BLbo, kTc5BLbo, 128);
+                    tc5_mma(d, ad, bd, tc5_idesc(32), (t | kk) != 0 ? 1u : 0u);
+                }
             }
         }
     }
     tc5_commit(c.bar);
+}
+
+// This thread's 16 accumulator columns (outputs 8 h .. 8 h + 7) of its vector: one block, or the sum of the three
+// stacked blocks.
+__device__ __forceinline__ void tc5_read(const Tc5& c, uint32_t taddr, float (&d)[16]) {
+    tmem_ld16(taddr, d);
+    if (c.stack) {
+        float e[16], f[16];
+        tmem_ld16(taddr + 32u, e);
+        tmem_ld16(taddr + 64u, f);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) d[i] = d[i] + e[i] + f[i];
+    }
 }
 
 // The tile's line FFT. Thread (warp w, lane l) owns vector v = 128 mb + 32 (w % 4) + l, mb = w / 8, and half h =
@@ -208,7 +253,7 @@ __device__ __forceinline__ bool tc5_fft(const float2* __restrict__ src, const fl
     auto row_of = [&](int jj) { return COLS ? jj * LINES + line : line * NV + jj; };  // vector (line, jj) -> A row
     uint8_t* a_blk = c.a_ptr;  // plane p of block b at (b * 3 + p) * kTc5Plane
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    const uint32_t d_col = c.tmem + lane_base + (uint32_t)mb * 32u + (uint32_t)h * 16u;
+    const uint32_t d_col = c.tmem + lane_base + (uint32_t)mb * tc5_block_cols(c.stack != 0) + (uint32_t)h * 16u;
 
     // ---- stage A: gather (radix-2 first stage folded in for R = 2), twiddle, split, write A rows ----
     {
@@ -248,7 +293,7 @@ __device__ __forceinline__ bool tc5_fft(const float2* __restrict__ src, const fl
     c.phase ^= 1u;
     tc_fence_after();
     float d[16];
-    if (ok) tmem_ld16(d_col, d);
+    if (ok) tc5_read(c, d_col, d);
     // ---- stage B: the outputs of stage A, twiddled for stage B and split, scattered into the A rows they feed ----
     // Output s = 8 h + i of stage A sits at (j - k) 16 + k + s NSA (k = j mod NSA) and is input rb of stage-B vector jb:
     // for R = 2, jb = k + 2 s and rb = j / 2; for R = 1, jb = s and rb = j. So along i the stage-B vector steps by
@@ -282,7 +327,7 @@ __device__ __forceinline__ bool tc5_fft(const float2* __restrict__ src, const fl
     ok = mbar_wait_bounded(c.bar, c.phase, kTc5WaitPolls) && ok;
     c.phase ^= 1u;
     tc_fence_after();
-    if (ok) tmem_ld16(d_col, d);
+    if (ok) tc5_read(c, d_col, d);
 #pragma unroll
     for (int i = 0; i < 8; ++i) z[i] = make_float2(d[2 * i], d[2 * i + 1]);
     tc_fence_before();

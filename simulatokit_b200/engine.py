@@ -38,7 +38,7 @@ class ExecutionOptions:
         self.col_tile = int(col_tile)
         self.tma = bool(tma)
         self.autotune = bool(autotune)
-        self.tcgen05 = bool(tcgen05)
+        self.tcgen05 = int(tcgen05)  # True / 1: twelve N = 32 products a stage, 2: six stacked ones, 0: mma.sync
         self.epilogue_detect = bool(epilogue_detect)
 
     @staticmethod
@@ -84,7 +84,7 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COL_TILE, o.col_tile))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TMA, 1 if o.tma else 0))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_AUTOTUNE, 1 if o.autotune else 0))
-        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TCGEN05, 1 if o.tcgen05 else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TCGEN05, int(o.tcgen05)))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_EPILOGUE_DETECT, 1 if o.epilogue_detect else 0))
 
     def set_stream(self, stream_ptr: int | None):

@@ -26,9 +26,10 @@ def _opts(form="bf16x3", tcgen05=True):
     return sk.ExecutionOptions(form=form, tcgen05=tcgen05)
 
 
-@pytest.mark.parametrize("tcgen05", [True, False])
+@pytest.mark.parametrize("tcgen05", [1, 2, 0])
 def test_hrtem_srtio3_exit_wave(engine, tcgen05):
-    """SrTiO3 4x4x5, 256^2, 10 slices of 1.9525 A, 200 keV plane wave, on either tensor-core engine."""
+    """SrTiO3 4x4x5, 256^2, 10 slices of 1.9525 A, 200 keV plane wave, on the tcgen05 engine (twelve or six stacked
+    products a stage) and on the mma.sync engine."""
     s = O.srtio3_cell().repeated(4, 4, 5)
     op = O.Potential.from_structure(s, 256, 256, slice_thickness=1.9525)
     og = op.grid
@@ -39,8 +40,8 @@ def test_hrtem_srtio3_exit_wave(engine, tcgen05):
                            engine=engine)[-1]
     e_wave = O.rel_l2(ex.field, ref)
     e_int = O.rel_l2(np.abs(ex.field) ** 2, np.abs(ref) ** 2)
-    print(f"bf16x3 ({'tcgen05' if tcgen05 else 'mma.sync'}) HRTEM 256^2 x 10 slices: exit wave rel-L2 {e_wave:.2e}, "
-          f"intensity {e_int:.2e}")
+    name = {1: "tcgen05", 2: "tcgen05 stacked", 0: "mma.sync"}[tcgen05]
+    print(f"bf16x3 ({name}) HRTEM 256^2 x 10 slices: exit wave rel-L2 {e_wave:.2e}, intensity {e_int:.2e}")
     assert e_wave <= 1e-4 and e_int <= 1e-4
     if tcgen05:  # three-term data split: float32-like accuracy
         assert e_wave <= 1e-5
@@ -71,6 +72,20 @@ def test_small_stem_scan_256(engine):
     print("rel-L2 vs float64 oracle (BF, HAADF):", errs)
     assert max(errs["bf16x3"]) <= 1e-4
     assert max(errs["fused"]) <= 1e-4
+
+
+def test_stacked_products_equal_the_twelve(engine):
+    """The six stacked products (N = 96, 64, 32) sum the same terms as the twelve of N = 32: a 512^2 scan agrees to
+    float32 rounding."""
+    s = O.srtio3_cell().repeated(4, 4, 6)
+    pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), 512, 512, slice_thickness=1.9525)
+    probe = sk.Probe(sk.ElectronBeam(200e3), pot.grid, sk.Aperture(20.0))
+    scan = sk.GridScan((3.905, 3.905), (2 * 3.905, 2 * 3.905), 4, 4)
+    dets = [sk.AnnularDetector(0, 20), sk.AnnularDetector(50, 120)]
+    a = sk.STEM.scan(probe, [pot], scan, dets, options=_opts(tcgen05=1), engine=engine)
+    b = sk.STEM.scan(probe, [pot], scan, dets, options=_opts(tcgen05=2), engine=engine)
+    for x, y in zip(a, b):
+        assert O.rel_l2(x.values, y.values) <= 1e-5
 
 
 def test_stem_scan_512_full_cell(engine):
