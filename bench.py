@@ -743,8 +743,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
-    ap.add_argument("--tcgen05", type=int, default=1, choices=[0, 1, 2],
-                    help="bf16x3 engine: 1 tcgen05 (twelve products a stage), 2 tcgen05 stacked (six), 0 mma.sync")
+    ap.add_argument("--tcgen05", type=int, default=2, choices=[0, 1, 2],
+                    help="bf16x3 engine: 2 tcgen05 stacked (six products a stage), 1 tcgen05 (twelve), 0 mma.sync")
     ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate", "jobs", "scanops", "tiling"],
                     help="stem: the headline STEM HAADF+BF scan; 4dstem, surrogate, jobs: the other configurations; "
                          "scanops: scan post-processing of a 4D-STEM measurement; tiling: the headline potential "
@@ -886,13 +886,13 @@ def main():
     # every form on the same scan (one timed scan each after a warm-up), for the metric's form comparison
     forms, form_values = {}, {}
     if rank == 0 and world == 1 and not args.no_forms:
-        # bf16x3: the tcgen05 engine (the form's default at this grid); bf16x3_stacked: the same with six stacked
-        # products a stage; bf16x3_mma_sync: the warp-level mma.sync stages
-        engines = {"bf16x3_stacked": 2, "bf16x3_mma_sync": 0}
-        for f in ("plain", "fused", "bf16x3", "bf16x3_stacked", "bf16x3_mma_sync"):
+        # bf16x3: the tcgen05 engine with six stacked products a stage (the form's default at this grid);
+        # bf16x3_twelve: the same terms as twelve products; bf16x3_mma_sync: the warp-level mma.sync stages
+        engines = {"bf16x3": 2, "bf16x3_twelve": 1, "bf16x3_mma_sync": 0}
+        for f in ("plain", "fused", "bf16x3", "bf16x3_twelve", "bf16x3_mma_sync"):
             engine.apply(sk.ExecutionOptions(form=f.split("_")[0], batch=args.batch, col_tile=args.col_tile,
                                              tma=not args.no_tma, autotune=args.autotune,
-                                             tcgen05=engines.get(f, 1)))
+                                             tcgen05=engines.get(f, 2)))
             engine.set_stream(stream.cuda_stream)
             scan_once()
             torch.cuda.synchronize()

@@ -54,9 +54,10 @@ extern "C" {
 #define SIMK_OPT_TUNED_TMA 10
 #define SIMK_OPT_TUNED_BATCH 11
 /* The bf16x3 form's radix-16 DFT stages on the fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
- * memory) for grid sides 256 and 512, with the data split in three BF16 terms: 1 (default) = twelve products of
- * N = 32 per block of 128 vectors; 2 = the same sums as six products of N = 96, 64 and 32 (the B terms stacked) whose
- * three accumulator blocks the threads add; 0 = the warp-level mma.sync stages (data in two terms) everywhere. */
+ * memory) for grid sides 256 and 512, with the data split in three BF16 terms: 2 (default) = six products of N = 96,
+ * 64 and 32 per block of 128 vectors (the B terms stacked) into three accumulator blocks, hi x hi alone in one, which
+ * the threads add; 1 = the same terms as twelve products of N = 32 into one accumulator; 0 = the warp-level mma.sync
+ * stages (data in two terms) everywhere. */
 #define SIMK_OPT_TCGEN05 12
 /* Sum the annular, centre-of-mass and segmented detectors inside the fused form's last column pass (TMA passes), so
  * the k-space waves are neither written nor read back unless a pixelated or binned detector wants them; 0 = detect

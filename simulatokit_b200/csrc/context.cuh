@@ -148,7 +148,7 @@ struct Context {
     int graphs = 1;
     int col_tile = 0;
     int tma = 1;            // TMA-pipelined persistent column pass where available
-    int tcgen05 = 1;        // the bf16x3 form's DFT stages on tcgen05 where its tiles fit (else mma.sync)
+    int tcgen05 = 2;        // the bf16x3 form's DFT stages on tcgen05 where its tiles fit (else mma.sync): 2 stacked
     int epilogue_detect = 1;  // channel detectors summed in the last column pass (TMA passes)
     int poisson_stream = 0;   // Poisson noise: 0 = a generator per value and sample, 1 = the reference's one stream
     int autotune = 0;       // time the launch configurations on first use of a (grid, form)

@@ -998,6 +998,30 @@ constexpr size_t tma_pass_smem(int n, int lines, int eng) {
                     : (eng != 0 ? 5 : 4) * (size_t)n * lines * sizeof(float2);
 }
 
+// Blocks of `kern` (threads, dynamic shared memory) that fit on one SM by its registers, shared memory, threads and
+// block slots, from the kernel's and the device's attributes. cudaOccupancyMaxActiveBlocksPerMultiprocessor reported
+// one block for the tcgen05 passes where two fit (101 KB of shared memory and 128 registers a thread; the profiler's
+// limits place two), so the persistent passes ask for the largest shared-memory carveout and take the larger of the
+// two figures. The passes' blocks never wait on one another, so a block that does not find room only starts later.
+int fitting_blocks(const void* kern, int threads, size_t dyn_smem, int device) {
+    cudaFuncAttributes fa;
+    SIMK_CUDA(cudaFuncGetAttributes(&fa, kern));
+    int regs = 0, smem = 0, reserved = 0, max_threads = 0, max_blocks = 0;
+    SIMK_CUDA(cudaDeviceGetAttribute(&regs, cudaDevAttrMaxRegistersPerMultiprocessor, device));
+    SIMK_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    SIMK_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
+    SIMK_CUDA(cudaDeviceGetAttribute(&max_threads, cudaDevAttrMaxThreadsPerMultiProcessor, device));
+    SIMK_CUDA(cudaDeviceGetAttribute(&max_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, device));
+    const int warps = (threads + 31) / 32;
+    const int regs_per_warp = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocated per warp in units of 256
+    const long long block_smem = (long long)fa.sharedSizeBytes + (long long)dyn_smem + reserved;
+    int n = max_blocks;
+    if (regs_per_warp > 0) n = std::min(n, regs / (regs_per_warp * warps));
+    if (block_smem > 0) n = (int)std::min<long long>(n, smem / block_smem);
+    n = std::min(n, max_threads / std::max(1, threads));
+    return std::max(0, n);
+}
+
 // Blocks per SM of a persistent pass: the occupancy, and for the tcgen05 engine at most what tensor memory holds.
 inline int pass_blocks_per_sm(int occupancy, int eng, int mb, bool stack) {
     if (eng == 3) occupancy = std::min(occupancy, 512 / (int)tc5_tmem_cols(mb, stack));
@@ -1018,7 +1042,9 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     static int occupancy = -1;
     if (occupancy < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, RB * T, smem));
+        occupancy = std::max(occupancy, fitting_blocks((const void*)kern, RB * T, smem, ctx.device));
     }
     const int stack = ctx.tcgen05 == 2 ? 1 : 0;
     const int blocks_per_sm = pass_blocks_per_sm(occupancy, ENG, ENG == 3 ? tc5_blocks(N, RB) : 0, stack != 0);
@@ -1046,7 +1072,9 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     static int occupancy = -1;
     if (occupancy < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, TC * T, smem));
+        occupancy = std::max(occupancy, fitting_blocks((const void*)kern, TC * T, smem, ctx.device));
     }
     const int stack = ctx.tcgen05 == 2 ? 1 : 0;
     const int blocks_per_sm = pass_blocks_per_sm(occupancy, ENG, ENG == 3 ? tc5_blocks(N, TC) : 0, stack != 0);

@@ -14,18 +14,21 @@
 // hi x lo2, hi x lo, lo x lo, lo2 x hi, lo x hi, hi x hi (A term x B term, small ones first); the dropped products are
 // below 2^-24 of the result. With a two-term data split the rounding of x_lo (2^-18 of x) is correlated across the
 // many equal values of a plane wave or a vacuum region and moved the total intensity by about 1e-5 per slice; with
-// three terms it is about 1e-8.
+// three terms it is about 1e-8. The tensor core's accumulator does not round to nearest when it adds a small product
+// to a large sum, so no product is added to hi x hi inside it: the twelve-instruction order adds hi x hi last, and
+// the stacked order keeps it in a column block of its own that the threads add in float32.
 //
 // Shared memory of a block: per block of 128 vectors three A planes (hi, lo, lo2), each K-major without swizzle: the
 // 16-byte chunk c (K = 8c .. 8c + 7, i.e. inputs r = 4c .. 4c + 3) of row v at c * kTc5Lbo + v * 16 (core matrices
 // of 8 rows x 16 bytes, 128 bytes apart along M: SBO = 128; chunks kTc5Lbo apart along K: LBO). kTc5Lbo = 2080 rather
 // than 2048 spreads the 4-byte scatter of the second stage over all 32 banks. Then the B operand of each direction:
-// the three terms' 32 rows stacked (rows 0-31 B_hi, 32-63 B_lo, 64-95 B_lo2), 4 chunks with LBO 1536, SBO 128, so
-// that one descriptor covers B_hi (N = 32), B_hi and B_lo (N = 64) or all three (N = 96).
+// the three terms' 32 rows stacked (rows 0-31 B_lo2, 32-63 B_lo, 64-95 B_hi), 4 chunks with LBO 1536, SBO 128, so
+// that one descriptor covers B_hi (N = 32, from row 64), B_lo and B_hi (N = 64, from row 32) or all three (N = 96).
 //
 // Products. Either twelve instructions of N = 32, each A term times each B term it pairs with accumulating into one
-// 32-column D (the default), or six of N = 96, 64, 32 (`stack`): A_hi times [B_hi B_lo B_lo2], A_lo times
-// [B_hi B_lo], A_lo2 times B_hi into three 32-column blocks of D, which the threads add as they read them.
+// 32-column D (the default), or six of N = 96, 64, 32 (`stack`): A_hi times [B_lo2 B_lo B_hi], A_lo times
+// [B_lo B_hi] and A_lo2 times B_hi into three 32-column blocks of D, (hi lo2 + lo lo + lo2 hi, hi lo + lo hi, hi hi),
+// which the threads add, the two small blocks first, as they read them.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -153,12 +156,12 @@ __device__ __forceinline__ void tc5_build_b(uint8_t* b, int tid, int nthreads) {
         const double r1 = val - (double)__bfloat162float(h);
         const __nv_bfloat16 l = __double2bfloat16(r1);
         const __nv_bfloat16 l2 = __double2bfloat16(r1 - (double)__bfloat162float(l));
-        // term t's row n sits at row 32 t + n of the direction's stacked matrix
+        // row n of B_lo2, B_lo, B_hi sits at row n, 32 + n, 64 + n of the direction's stacked matrix
         const uint32_t off = (uint32_t)(k >> 3) * kTc5BLbo + (uint32_t)n * 16u + (uint32_t)(k & 7) * 2u;
         uint8_t* bd = b + inv * kTc5BBytes + off;
-        *reinterpret_cast<__nv_bfloat16*>(bd) = h;
+        *reinterpret_cast<__nv_bfloat16*>(bd) = l2;
         *reinterpret_cast<__nv_bfloat16*>(bd + 32 * 16) = l;
-        *reinterpret_cast<__nv_bfloat16*>(bd + 64 * 16) = l2;
+        *reinterpret_cast<__nv_bfloat16*>(bd + 64 * 16) = h;
     }
 }
 
@@ -173,21 +176,23 @@ __device__ __forceinline__ void tc5_issue(const Tc5& c) {
     for (int mb = 0; mb < MB; ++mb) {
         const uint32_t d = c.tmem + (uint32_t)mb * bcols;
         if (c.stack) {
-            // A_hi x [B_hi B_lo B_lo2] (N = 96, initialises all three blocks), A_lo x [B_hi B_lo], A_lo2 x B_hi
+            // A_hi x [B_lo2 B_lo B_hi] (N = 96 from row 0, initialises all three blocks), A_lo x [B_lo B_hi] (N = 64
+            // from row 32), A_lo2 x B_hi (N = 32 from row 64), every one into the blocks from column 0
 #pragma unroll
             for (int pa = 0; pa < 3; ++pa) {
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     const uint64_t ad = tc5_desc(c.a_base + (uint32_t)(mb * 3 + pa) * kTc5Plane + 2u * kk * kTc5Lbo,
                                                  kTc5Lbo, 128);
-                    const uint64_t bd = tc5_desc(bbase + 2u * kk * kTc5BLbo, kTc5BLbo, 128);
+                    const uint64_t bd =
+                        tc5_desc(bbase + (uint32_t)pa * 32u * 16u + 2u * kk * kTc5BLbo, kTc5BLbo, 128);
                     tc5_mma(d, ad, bd, tc5_idesc(96u - 32u * (uint32_t)pa), (pa | kk) != 0 ? 1u : 0u);
                 }
             }
         } else {
-            // (A plane, B term): hi x lo2, hi x lo, lo x lo, lo2 x hi, lo x hi, hi x hi into one 32-column D
+            // (A plane, B row block): hi x lo2, hi x lo, lo x lo, lo2 x hi, lo x hi, hi x hi into one 32-column D
             constexpr int pa[6] = {0, 0, 1, 2, 1, 0};
-            constexpr int tb[6] = {2, 1, 1, 0, 0, 0};
+            constexpr int tb[6] = {0, 1, 1, 2, 2, 2};
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
 #pragma unroll
@@ -204,7 +209,7 @@ __device__ __forceinline__ void tc5_issue(const Tc5& c) {
 }
 
 // This thread's 16 accumulator columns (outputs 8 h .. 8 h + 7) of its vector: one block, or the sum of the three
-// stacked blocks.
+// stacked blocks, the two small ones first.
 __device__ __forceinline__ void tc5_read(const Tc5& c, uint32_t taddr, float (&d)[16]) {
     tmem_ld16(taddr, d);
     if (c.stack) {
@@ -212,7 +217,7 @@ __device__ __forceinline__ void tc5_read(const Tc5& c, uint32_t taddr, float (&d
         tmem_ld16(taddr + 32u, e);
         tmem_ld16(taddr + 64u, f);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) d[i] = d[i] + e[i] + f[i];
+        for (int i = 0; i < 16; ++i) d[i] = (d[i] + e[i]) + f[i];
     }
 }
 

@@ -21,13 +21,14 @@ class ExecutionOptions:
     the fused column pass (0 = automatic). tma: the TMA-pipelined persistent column pass where available. autotune:
     time the column tile, TMA passes and batch size on the first fused scan of a grid and use the fastest where the
     settings above are automatic. tcgen05: the bf16x3 form's DFT stages on the fifth-generation tensor cores
-    (tcgen05.mma, tensor-memory accumulators) at grid sides 256 and 512; False keeps the warp-level mma.sync stages.
+    (tcgen05.mma, tensor-memory accumulators) at grid sides 256 and 512: 2 (default) six stacked products a stage,
+    1 twelve products of N = 32, 0 / False the warp-level mma.sync stages.
     epilogue_detect: sum the channel detectors inside the last column pass (TMA passes) instead of separate kernels."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
     def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
-                 col_tile: int = 0, tma: bool = True, autotune: bool = False, tcgen05: bool = True,
+                 col_tile: int = 0, tma: bool = True, autotune: bool = False, tcgen05: int = 2,
                  epilogue_detect: bool = True):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
@@ -38,7 +39,7 @@ class ExecutionOptions:
         self.col_tile = int(col_tile)
         self.tma = bool(tma)
         self.autotune = bool(autotune)
-        self.tcgen05 = int(tcgen05)  # True / 1: twelve N = 32 products a stage, 2: six stacked ones, 0: mma.sync
+        self.tcgen05 = int(tcgen05)  # 2: six stacked products a stage, 1 / True: twelve of N = 32, 0: mma.sync
         self.epilogue_detect = bool(epilogue_detect)
 
     @staticmethod

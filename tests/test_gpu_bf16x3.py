@@ -22,13 +22,13 @@ def engine():
     return sk.Engine.require()
 
 
-def _opts(form="bf16x3", tcgen05=True):
+def _opts(form="bf16x3", tcgen05=2):
     return sk.ExecutionOptions(form=form, tcgen05=tcgen05)
 
 
-@pytest.mark.parametrize("tcgen05", [1, 2, 0])
+@pytest.mark.parametrize("tcgen05", [2, 1, 0])
 def test_hrtem_srtio3_exit_wave(engine, tcgen05):
-    """SrTiO3 4x4x5, 256^2, 10 slices of 1.9525 A, 200 keV plane wave, on the tcgen05 engine (twelve or six stacked
+    """SrTiO3 4x4x5, 256^2, 10 slices of 1.9525 A, 200 keV plane wave, on the tcgen05 engine (six stacked or twelve
     products a stage) and on the mma.sync engine."""
     s = O.srtio3_cell().repeated(4, 4, 5)
     op = O.Potential.from_structure(s, 256, 256, slice_thickness=1.9525)
@@ -76,7 +76,8 @@ def test_small_stem_scan_256(engine):
 
 def test_stacked_products_equal_the_twelve(engine):
     """The six stacked products (N = 96, 64, 32) sum the same terms as the twelve of N = 32: a 512^2 scan agrees to
-    float32 rounding."""
+    float32 rounding. (With hi x hi first in a stacked accumulator block, the small terms added to it inside the
+    tensor core lost low bits and the two differed by 1.7e-5; it now has a block of its own.)"""
     s = O.srtio3_cell().repeated(4, 4, 6)
     pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), 512, 512, slice_thickness=1.9525)
     probe = sk.Probe(sk.ElectronBeam(200e3), pot.grid, sk.Aperture(20.0))
