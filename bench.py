@@ -712,7 +712,7 @@ def run_extra(args):
     torch.cuda.set_stream(stream)
     engine.set_stream(stream.cuda_stream)
     engine.apply(sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma,
-                             autotune=args.autotune))
+                                     autotune=args.autotune, tcgen05=args.tcgen05, composite=bool(args.composite)))
     fn = {"4dstem": run_4dstem, "surrogate": run_surrogate, "jobs": run_jobs, "scanops": run_scanops,
           "tiling": run_tiling}[args.workload]
     line = fn(args, sk, L, engine, stream, torch, local)
@@ -743,6 +743,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
+    ap.add_argument("--composite", type=int, default=1, choices=[0, 1],
+                    help="fused passes at 3 or 5 times a power of two: 1 composite register engine, 0 shared-memory")
     ap.add_argument("--tcgen05", type=int, default=2, choices=[0, 1, 2],
                     help="bf16x3 engine: 2 tcgen05 stacked (six products a stage), 1 tcgen05 (twelve), 0 mma.sync")
     ap.add_argument("--workload", default="stem", choices=["stem", "4dstem", "surrogate", "jobs", "scanops", "tiling"],
@@ -785,7 +787,7 @@ def main():
     assert stream.cuda_stream != 0
     engine.set_stream(stream.cuda_stream)
     opts = sk.ExecutionOptions(form=args.form, batch=args.batch, col_tile=args.col_tile, tma=not args.no_tma,
-                               autotune=args.autotune, tcgen05=args.tcgen05)
+                               autotune=args.autotune, tcgen05=args.tcgen05, composite=bool(args.composite))
     engine.apply(opts)
 
     box, nums, pos = srtio3(8, 8, 20)

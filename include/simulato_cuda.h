@@ -68,6 +68,10 @@ extern "C" {
  * single GaussianGenerator stream over the samples and values in order (ScanOperations.swift:80-117), walked by one
  * device thread, so a seed gives the reference's draws. */
 #define SIMK_OPT_POISSON_STREAM 14
+/* The fused form's passes at lengths 3 or 5 times a power of two (384, 640, 768, 1536): 1 (default) = the composite
+ * register engine (each line as 3 or 5 register-resident power-of-two transforms of its decimated sub-lines); 0 = the
+ * shared-memory Stockham engine. */
+#define SIMK_OPT_COMPOSITE 15
 
 /* ---- Lobato pi choice (LobatoParameterization.PiConstant, LobatoParameterization.swift:15-24) ---- */
 #define SIMK_PI_EXACT 0

@@ -162,6 +162,7 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                 SIMK_REQUIRE(value == 0 || value == 1, "Poisson stream must be 0 (per value) or 1 (reference order)");
                 c.poisson_stream = (int)value;
                 break;
+            case SIMK_OPT_COMPOSITE: c.composite = value ? 1 : 0; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -206,6 +207,7 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_TCGEN05: *value = c.tcgen05; break;
             case SIMK_OPT_EPILOGUE_DETECT: *value = c.epilogue_detect; break;
             case SIMK_OPT_POISSON_STREAM: *value = c.poisson_stream; break;
+            case SIMK_OPT_COMPOSITE: *value = c.composite; break;
             case SIMK_OPT_TUNED_COL_TILE: *value = c.last_tuned.col_tile; break;
             case SIMK_OPT_TUNED_TMA: *value = c.last_tuned.tma; break;
             case SIMK_OPT_TUNED_BATCH: *value = c.last_tuned.batch; break;

@@ -151,6 +151,7 @@ struct Context {
     int tcgen05 = 2;        // the bf16x3 form's DFT stages on tcgen05 where its tiles fit (else mma.sync): 2 stacked
     int epilogue_detect = 1;  // channel detectors summed in the last column pass (TMA passes)
     int poisson_stream = 0;   // Poisson noise: 0 = a generator per value and sample, 1 = the reference's one stream
+    int composite = 1;        // fused passes at 3 or 5 times a power of two: the composite register engine
     int autotune = 0;       // time the launch configurations on first use of a (grid, form)
     struct Tuned {
         int col_tile = -1, tma = -1;

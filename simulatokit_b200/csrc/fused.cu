@@ -237,7 +237,8 @@ template <int N> struct TwRegs {
     float2 w[Pow2<N>::NP > 1 ? Pow2<N>::NP - 1 : 1][7];
 };
 
-template <int N, int F>
+// `tw` holds W_{N S}^m (S > 1: the table of a length that N divides; W_N^m = W_{N S}^{m S}).
+template <int N, int F, int S = 1>
 __device__ __forceinline__ void tw_load(TwRegs<N>& tr, unsigned t, const float2* __restrict__ tw) {
     using P = Pow2<N>;
     if constexpr (F < P::NP) {
@@ -246,9 +247,9 @@ __device__ __forceinline__ void tw_load(TwRegs<N>& tr, unsigned t, const float2*
         for (int q = 0; q < Q; ++q) {
             const unsigned k = (t + P::T * q) & (NS - 1);
 #pragma unroll
-            for (int r = 1; r < R; ++r) tr.w[F - 1][q * (R - 1) + r - 1] = __ldg(tw + k * (r * TSTRIDE));
+            for (int r = 1; r < R; ++r) tr.w[F - 1][q * (R - 1) + r - 1] = __ldg(tw + k * (r * TSTRIDE) * S);
         }
-        tw_load<N, F + 1>(tr, t, tw);
+        tw_load<N, F + 1, S>(tr, t, tw);
     }
 }
 
@@ -301,6 +302,80 @@ __device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const Tw
             line_sync<LT>(bar_id);
         }
         ct_fft_from<N, F + 1, DIR, STRIDE, LT>(v, t, tr, sm, bar_id);
+    }
+}
+
+// ---- composite lengths N = R M (R = 3 or 5, M a power of two >= 64): the register engine on R sub-lines ---------------
+// A line's N / 8 threads form R sub-lines of TS = M / 8 threads; thread (g, u) is sub-line g, thread u. Decimation in
+// frequency from natural order (comp_dif_in, then the M-point register transform of each sub-line):
+//     X[R k1 + g] = sum_{n1} W_M^{n1 k1} y_g[n1],   y_g[n1] = W_N^{n1 g} sum_{n2} x[n1 + M n2] W_R^{n2 g},
+// so thread (g, u) ends with X[R (u + TS i) + g] in v[i]. Decimation in time back to natural order: the M-point
+// transform of X[R . + g] (v in that order), w_g[n1] = W_N^{n1 g} z_g[n1] into an exchange tile (comp_dit_twiddle),
+// and after the line's barrier x[n1 + M g] = sum_{k2} W_R^{g k2} w_{k2}[n1] (comp_dit_out). Every W is taken in the
+// transform's direction; the R-point sums are the butterflies of fft.cuh with output g selected.
+template <int N> struct CompPlan {
+    static constexpr int R = (N % 3 == 0) ? 3 : 5;
+    static constexpr int M = N / R;
+    static constexpr int TS = M / 8;
+};
+constexpr bool comp_length(int n) {
+    for (int r : {3, 5}) {
+        if (n % r) continue;
+        const int m = n / r;
+        if (m >= 64 && (m & (m - 1)) == 0) return true;
+    }
+    return false;
+}
+template <int R, int DIR> __device__ __forceinline__ float2 comp_dft_out(float2 (&x)[R], int g) {
+    if constexpr (R == 3) bfly3<DIR>(x);
+    else bfly5<DIR>(x);
+    float2 y = x[0];
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+        if (g == r) y = x[r];
+    return y;
+}
+// ld(idx): element idx of the line in natural order; tw: the N-entry table W_N^m.
+template <int N, int DIR, typename Ld>
+__device__ __forceinline__ void comp_dif_in(float2 (&v)[8], int g, int u, const float2* __restrict__ tw, Ld&& ld) {
+    using C = CompPlan<N>;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int n1 = u + C::TS * i;
+        float2 x[C::R];
+#pragma unroll
+        for (int r = 0; r < C::R; ++r) x[r] = ld(n1 + C::M * r);
+        const float2 y = comp_dft_out<C::R, DIR>(x, g);
+        const float2 w = __ldg(tw + n1 * g);  // n1 g < M R = N
+        v[i] = (DIR < 0) ? cmul(y, w) : cmulc(y, w);
+        // keeps the next point's loads after this one: hoisting all R * 8 loads spills under the register cap
+        asm volatile("" ::: "memory");
+    }
+}
+// st(slot, value): slot g M + n1 of the exchange tile.
+template <int N, int DIR, typename St>
+__device__ __forceinline__ void comp_dit_twiddle(const float2 (&v)[8], int g, int u, const float2* __restrict__ tw,
+                                                 St&& st) {
+    using C = CompPlan<N>;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int n1 = u + C::TS * i;
+        const float2 w = __ldg(tw + n1 * g);
+        st(g * C::M + n1, (DIR < 0) ? cmul(v[i], w) : cmulc(v[i], w));
+    }
+}
+// ld(slot): slot k2 M + n1 of the exchange tile; v[i] = x[u + TS i + M g].
+template <int N, int DIR, typename Ld>
+__device__ __forceinline__ void comp_dit_out(float2 (&v)[8], int g, int u, Ld&& ld) {
+    using C = CompPlan<N>;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int n1 = u + C::TS * i;
+        float2 x[C::R];
+#pragma unroll
+        for (int r = 0; r < C::R; ++r) x[r] = ld(r * C::M + n1);
+        v[i] = comp_dft_out<C::R, DIR>(x, g);
+        asm volatile("" ::: "memory");  // as in comp_dif_in
     }
 }
 
@@ -453,10 +528,12 @@ constexpr int rows_per_tile(int n) {
 }
 
 // State an engine keeps per thread: register twiddles (0), the DFT-16 fragments (1), nothing (2), the tcgen05 block
-// state (3).
+// state (3), the sub-lines' register twiddles (4).
 template <int N, int ENG>
-using EngineState = std::conditional_t<ENG == 0, TwRegs<N>,
-                                       std::conditional_t<ENG == 1, Dft16Frags, std::conditional_t<ENG == 3, Tc5, int>>>;
+using EngineState = std::conditional_t<
+    ENG == 0, TwRegs<N>,
+    std::conditional_t<ENG == 1, Dft16Frags,
+                       std::conditional_t<ENG == 3, Tc5, std::conditional_t<ENG == 4, TwRegs<CompPlan<N>::M>, int>>>>;
 
 // The tcgen05 engine (3) takes lines of 256 and 512 points in tiles of whole 128-vector blocks.
 constexpr bool tc5_tile(int n, int lines) { return (n == 256 || n == 512) && (n * lines) % 2048 == 0; }
@@ -504,10 +581,14 @@ __device__ __forceinline__ void tc5_release(const Tc5& c, int tid, bool aborted)
 // Blocks per SM the engines ask the compiler for. The tensor-core engine: two when a block has at most 256 threads
 // (at most 128 registers a thread). The float32 register engine: three for its 256-thread blocks (at most 85
 // registers; 512^2 fits without spills and gains a third block per SM). The float32 shared-memory engine keeps the
-// compiler's choice (capped at 84 registers it spilled and lost 12 % at 768^2).
+// compiler's choice (capped at 84 registers it spilled and lost 12 % at 768^2). The composite-length register engine:
+// two blocks of up to 384 threads (80 registers; the 768^2 column pass spills 84 bytes and is still the fastest
+// choice measured, 0.86 ms a launch against 0.90 ms for one block at 168 registers), three of up to 256 threads (112
+// registers: the row pass spilled 240 bytes at four blocks and 80 registers and ran 6 % slower).
 constexpr int tc_min_blocks(int threads, int eng) {
     if (eng == 1 || eng == 3) return threads <= 256 ? 2 : 1;
     if (eng == 0) return threads == 256 ? 3 : 1;
+    if (eng == 4) return threads <= 256 ? 3 : (threads <= 384 ? 2 : 1);
     return 1;
 }
 
@@ -544,6 +625,7 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     __syncthreads();
     [[maybe_unused]] EngineState<N, ENG> eng;
     if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
+    else if constexpr (ENG == 4) tw_load<CompPlan<N>::M, 1, CompPlan<N>::R>(eng, t % CompPlan<N>::TS, tw);
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     else if constexpr (ENG == 3)
         eng = tc5_setup<tc5_blocks(N, TC)>(smem_tma + 4 * (size_t)TILE * sizeof(float2), &tmem_slot, &mma_bar, tid,
@@ -596,6 +678,33 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
 #pragma unroll
             for (int i = 0; i < 8; ++i) buf[(t + T * i) * TC + c] = v[i];
             store_src = buf;
+        } else if constexpr (ENG == 4) {
+            // composite length: R sub-lines of TS threads per column; a sub-line's exchanges use its own part of the
+            // wave tile and synchronise the TC TS threads of sub-line g (whole warps: threads t = TS g .. of every
+            // column), with the named barrier 1 + g
+            using C = CompPlan<N>;
+            const int g = (int)t / C::TS, u = (int)t % C::TS;
+            float2 v[8];
+            comp_dif_in<N, -1>(v, g, u, tw, [&](int idx) { return buf[idx * TC + c]; });
+            __syncthreads();  // every sub-line has read the wave tile: its parts become the exchange buffers
+            const SmemCT<TC> sm{buf + g * C::M * TC + c};
+            ct_fft_from<C::M, 0, -1, TC, C::TS * TC>(v, (unsigned)u, eng, sm, 1 + g);
+            float2* out = buf + TILE;  // the P tile takes the result once every thread has multiplied by it
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int idx = C::R * (u + C::TS * i) + g;  // v[i] = X[idx]
+                v[i] = cmul(v[i], pbuf[idx * TC + c]) * pscale;
+                if constexpr (MODE != 0) out[idx * TC + c] = v[i];  // each slot is read and written by its thread
+            }
+            if constexpr (MODE == 0) {
+                ct_fft_from<C::M, 0, +1, TC, C::TS * TC>(v, (unsigned)u, eng, sm, 1 + g);
+                comp_dit_twiddle<N, +1>(v, g, u, tw, [&](int slot, float2 x) { buf[slot * TC + c] = x; });
+                __syncthreads();  // the sub-lines' twiddled transforms are in the wave tile; P has been read
+                comp_dit_out<N, +1>(v, g, u, [&](int slot) { return buf[slot * TC + c]; });
+#pragma unroll
+                for (int i = 0; i < 8; ++i) out[(u + C::TS * i + C::M * g) * TC + c] = v[i];
+            }
+            store_src = out;
         } else if constexpr (ENG == 2) {
             using L = CcLayout<N, TC, true>;
             float2* scratch = stages + 4 * TILE;
@@ -663,8 +772,10 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             bulk_commit();
         }
         if constexpr (MODE == 3) {
-            // the P tile has been read: its space holds the warps' sums (TILE float2 >= NT / 32 * C doubles, C <= 64)
-            detect_tile<TC * T>(store_src, det, b, (iy - c) / TC, tid, reinterpret_cast<double*>(buf + TILE));
+            // the tile the result is not in holds the warps' sums (TILE float2 >= NT / 32 * C doubles, C <= 64): the P
+            // tile (read by now), or for the composite engine, whose result is in the P tile, the wave tile
+            float2* sums = (ENG == 4) ? buf : buf + TILE;
+            detect_tile<TC * T>(store_src, det, b, (iy - c) / TC, tid, reinterpret_cast<double*>(sums));
             fence_proxy_async_shared();  // the sums were written by this proxy; the next copy into the stage by TMA
             __syncthreads();  // the partials' reads of the tile and of the sums precede the next copy into the stage
         }
@@ -704,15 +815,17 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
     __syncthreads();
     [[maybe_unused]] EngineState<N, ENG> eng;
     if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
+    else if constexpr (ENG == 4) tw_load<CompPlan<N>::M, 1, CompPlan<N>::R>(eng, t % CompPlan<N>::TS, tw);
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     else if constexpr (ENG == 3)
         eng = tc5_setup<tc5_blocks(N, RB)>(smem_rtma + 4 * (size_t)TILE * sizeof(float2), &tmem_slot, &mma_bar, tid,
                                            RB * T, tc5_stack);
-    constexpr bool kStoreFromStage = (ENG == 0 || ENG == 3);  // the finished rows go back by a bulk store
+    // the finished rows go back by a bulk store from the stage: its wave rows (ENG 0, 3) or its rows of t (ENG 4)
+    constexpr bool kStoreFromStage = (ENG == 0 || ENG == 3 || ENG == 4);
     auto issue = [&](int tile, int s) {
         float2* dst = stages + s * 2 * TILE;
         const int row0 = tile * RB;
-        // ENG 0 and 3 store each tile from its stage: the previous tile's store must have read the stage first
+        // ENG 0, 3 and 4 store each tile from its stage: the previous tile's store must have read the stage first
         if constexpr (kStoreFromStage) bulk_wait_read();
         mbar_arrive_expect_tx(&full[s], with_t ? 2 * bytes : bytes);
         bulk_load(dst, psi + (size_t)row0 * N, bytes, &full[s]);
@@ -758,6 +871,60 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
             // barrier below
 #pragma unroll
             for (int i = 0; i < 8; ++i) buf[rr * N + t + T * i] = v[i];
+        } else if constexpr (ENG == 4) {
+            // composite length: R sub-lines of TS threads per row. The row's barrier: its T threads (named 1 + rr)
+            // when they are whole warps and the tile has several rows, else the block; a sub-line's: __syncwarp when
+            // it lies in one warp, else the named barrier 1 + RB + R rr + g
+            using C = CompPlan<N>;
+            constexpr int LT = (RB > 1 && T % 32 == 0 && RB < 16) ? T : 0;
+            constexpr int LS = C::TS <= 32 ? 32 : C::TS;
+            static_assert(LS == 32 || RB + RB * C::R <= 15, "named barriers 1..15");
+            const int g = (int)t / C::TS, u = (int)t % C::TS;
+            const int line_bar = 1 + rr, sub_bar = 1 + RB + rr * C::R + g;
+            float2* line = buf + rr * N;
+            float2* tout = buf + TILE + rr * N;  // the row's part of the t tile takes the result
+            const float2* trow = tbuf + rr * N;
+            float2 v[8];
+            if (inv || fwd) {
+                if (inv) {
+                    comp_dif_in<N, +1>(v, g, u, tw, [&](int idx) { return line[idx]; });
+                } else if (with_t) {  // the forward transform alone: t multiplies the row before it
+                    comp_dif_in<N, -1>(v, g, u, tw, [&](int idx) { return cmul(line[idx], trow[idx]) * scale; });
+                } else {
+                    comp_dif_in<N, -1>(v, g, u, tw, [&](int idx) { return line[idx] * scale; });
+                }
+                line_sync<LT>(line_bar);  // the row has been read: its sub-line parts become exchange buffers
+                const SmemCT<0> sm{line + g * C::M};
+                if (inv) {
+                    ct_fft_from<C::M, 0, +1, 0, LS>(v, (unsigned)u, eng, sm, sub_bar);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int idx = C::R * (u + C::TS * i) + g;  // v[i] = element idx
+                        v[i] = with_t ? cmul(v[i], trow[idx]) * scale : v[i] * scale;
+                    }
+                } else {
+                    ct_fft_from<C::M, 0, -1, 0, LS>(v, (unsigned)u, eng, sm, sub_bar);
+                }
+                if (inv && fwd) {
+                    ct_fft_from<C::M, 0, -1, 0, LS>(v, (unsigned)u, eng, sm, sub_bar);
+                    comp_dit_twiddle<N, -1>(v, g, u, tw, [&](int slot, float2 x) { line[slot] = x; });
+                    line_sync<LT>(line_bar);  // the sub-lines' twiddled transforms are in the row; t has been read
+                    comp_dit_out<N, -1>(v, g, u, [&](int slot) { return line[slot]; });
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) tout[u + C::TS * i + C::M * g] = v[i];
+                } else {
+                    // one transform: element R k1 + g in v, read (inverse) or no longer read (forward) at that slot
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) tout[C::R * (u + C::TS * i) + g] = v[i];
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int idx = (int)t + T * i;
+                    v[i] = with_t ? cmul(line[idx], trow[idx]) * scale : line[idx] * scale;
+                    tout[idx] = v[i];
+                }
+            }
         } else if constexpr (ENG == 3) {
             constexpr int NV = N / 16;
             float2 z[8];
@@ -843,7 +1010,7 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
         __syncthreads();  // every thread is done with the stage before its next copy
         if constexpr (kStoreFromStage) {
             if (tid == 0) {
-                bulk_store(psi + (size_t)tile * RB * N, buf, bytes);
+                bulk_store(psi + (size_t)tile * RB * N, ENG == 4 ? buf + TILE : buf, bytes);
                 bulk_commit();
             }
         }
@@ -995,7 +1162,7 @@ void ensure_err_flag(Context& ctx) {
 // tile (1, 2) or the tcgen05 engine's operands (3).
 constexpr size_t tma_pass_smem(int n, int lines, int eng) {
     return eng == 3 ? 4 * (size_t)n * lines * sizeof(float2) + tc5_smem_bytes(tc5_blocks(n, lines))
-                    : (eng != 0 ? 5 : 4) * (size_t)n * lines * sizeof(float2);
+                    : (eng != 0 && eng != 4 ? 5 : 4) * (size_t)n * lines * sizeof(float2);
 }
 
 // Blocks of `kern` (threads, dynamic shared memory) that fit on one SM by its registers, shared memory, threads and
@@ -1251,15 +1418,37 @@ bool cols_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
     }
 }
 
-// ---- the float32 fused form at lengths that are not powers of two: the TMA passes with the shared-memory engine -----
+// ---- the float32 fused form at lengths that are not powers of two: the TMA passes with the composite-length register
+// engine (4) where N = 3 or 5 times a power of two, else the shared-memory engine (2); SIMK_OPT_COMPOSITE = 0 keeps 2 ---
+template <int N>
+bool rows_cc_n(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
+               int fwd, float scale) {
+    if constexpr (comp_length(N)) {
+        if (ctx.composite && launch_rows_tma<N, 4>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale)) return true;
+    }
+    return launch_rows_tma<N, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+}
+
 bool rows_cc(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv, int fwd,
              float scale) {
     switch (p.n) {
-        case 384: return launch_rows_tma<384, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
-        case 640: return launch_rows_tma<640, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
-        case 768: return launch_rows_tma<768, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
-        case 1536: return launch_rows_tma<1536, 2>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 384: return rows_cc_n<384>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 640: return rows_cc_n<640>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 768: return rows_cc_n<768>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
+        case 1536: return rows_cc_n<1536>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
         default: return false;
+    }
+}
+
+template <int N, int TC>
+bool cols_cc_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count) {
+    if constexpr (TC * (N / 8) > 1024) {
+        return false;
+    } else {
+        if constexpr (comp_length(N)) {
+            if (ctx.composite && launch_cols_tma<N, TC, 4>(ctx, p, a, count)) return true;
+        }
+        return launch_cols_tma<N, TC, 2>(ctx, p, a, count);
     }
 }
 
@@ -1267,19 +1456,9 @@ template <int N>
 bool cols_cc_n(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
     for (; tc >= 2; tc /= 2) {
         switch (tc) {
-            case 8:
-                if constexpr (8 * (N / 8) <= 1024) {
-                    if (launch_cols_tma<N, 8, 2>(ctx, p, a, count)) return true;
-                }
-                break;
-            case 4:
-                if constexpr (4 * (N / 8) <= 1024) {
-                    if (launch_cols_tma<N, 4, 2>(ctx, p, a, count)) return true;
-                }
-                break;
-            case 2:
-                if (launch_cols_tma<N, 2, 2>(ctx, p, a, count)) return true;
-                break;
+            case 8: if (cols_cc_tc<N, 8>(ctx, p, a, count)) return true; break;
+            case 4: if (cols_cc_tc<N, 4>(ctx, p, a, count)) return true; break;
+            case 2: if (cols_cc_tc<N, 2>(ctx, p, a, count)) return true; break;
             default: break;
         }
     }
@@ -1429,6 +1608,7 @@ int propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, 
     key_append(key, ctx.col_tile);
     key_append(key, ctx.tma);
     key_append(key, ctx.tcgen05);
+    key_append(key, ctx.composite);
     key_append(key, ctx.stream);
     const FusedDetect nodet{};
     const FusedDetect& d = det ? *det : nodet;

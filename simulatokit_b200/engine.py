@@ -23,13 +23,16 @@ class ExecutionOptions:
     settings above are automatic. tcgen05: the bf16x3 form's DFT stages on the fifth-generation tensor cores
     (tcgen05.mma, tensor-memory accumulators) at grid sides 256 and 512: 2 (default) six stacked products a stage,
     1 twelve products of N = 32, 0 / False the warp-level mma.sync stages.
-    epilogue_detect: sum the channel detectors inside the last column pass (TMA passes) instead of separate kernels."""
+    epilogue_detect: sum the channel detectors inside the last column pass (TMA passes) instead of separate kernels.
+    composite: at grid sides 3 or 5 times a power of two (384, 640, 768, 1536) the fused passes transform each line as
+    register-resident power-of-two transforms of its decimated sub-lines; False keeps the shared-memory Stockham
+    engine."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
     def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
                  col_tile: int = 0, tma: bool = True, autotune: bool = False, tcgen05: int = 2,
-                 epilogue_detect: bool = True):
+                 epilogue_detect: bool = True, composite: bool = True):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
         self.form = form
@@ -41,6 +44,7 @@ class ExecutionOptions:
         self.autotune = bool(autotune)
         self.tcgen05 = int(tcgen05)  # 2: six stacked products a stage, 1 / True: twelve of N = 32, 0: mma.sync
         self.epilogue_detect = bool(epilogue_detect)
+        self.composite = bool(composite)
 
     @staticmethod
     def standard() -> "ExecutionOptions":
@@ -87,6 +91,7 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_AUTOTUNE, 1 if o.autotune else 0))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TCGEN05, int(o.tcgen05)))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_EPILOGUE_DETECT, 1 if o.epilogue_detect else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COMPOSITE, 1 if o.composite else 0))
 
     def set_stream(self, stream_ptr: int | None):
         L.check(self.lib.simk_context_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))

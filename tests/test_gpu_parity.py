@@ -261,10 +261,12 @@ def test_refusals(engine):
         sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), other), pot, engine=engine)
 
 
+@pytest.mark.parametrize("composite", [True, False])
 @pytest.mark.parametrize("nx,ny", [(384, 384), (640, 384), (768, 768), (1536, 1536)])
-def test_fused_mixed_radix_lengths(engine, nx, ny):
-    """The fused form's TMA passes with the float32 shared-memory engine (radix 8/4/2 then 3 or 5) at grid sides that
-    are not powers of two: exit wave of a plane wave through SrTiO3 2x2x2 (4 slices) <= 1e-5 relative L2."""
+def test_fused_mixed_radix_lengths(engine, nx, ny, composite):
+    """The fused form's TMA passes at grid sides that are not powers of two, on the composite register engine (each line
+    as 3 or 5 register-resident power-of-two transforms of its decimated sub-lines) and on the float32 shared-memory
+    engine (radix 8/4/2 then 3 or 5): exit wave of a plane wave through SrTiO3 2x2x2 (4 slices) <= 1e-5 relative L2."""
     s = O.srtio3_cell().repeated(2, 2, 2)
     op = O.Potential.from_structure(s, nx, ny, slice_thickness=1.9525)
     og = op.grid
@@ -272,5 +274,32 @@ def test_fused_mixed_radix_lengths(engine, nx, ny):
     ref = O.multislice(O.plane_wave(og), ts, op.thicknesses, 200e3, og)[-1]
     pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), nx, ny, slice_thickness=1.9525)
     ex = sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), pot.grid), pot,
-                           options=sk.ExecutionOptions(form="fused"), engine=engine)[-1]
+                           options=sk.ExecutionOptions(form="fused", composite=composite), engine=engine)[-1]
     assert O.rel_l2(ex.field, ref) <= 1e-5
+
+
+@pytest.mark.parametrize("n,col_tile", [(768, 4), (768, 2), (384, 8), (640, 4)])
+def test_composite_engine_scan(engine, n, col_tile):
+    """A probe scan at a side 3 or 5 times a power of two on the composite register engine: the probes' row passes,
+    the slices' row and column passes and the last column pass with the detectors in its epilogue (annular, centre of
+    mass) against the float64 oracle (annular <= 1e-4, centre of mass <= 1e-3 relative L2) and against the
+    shared-memory engine (annular <= 5e-6, centre of mass <= 1e-4)."""
+    s = O.srtio3_cell().repeated(2, 2, 2)
+    st = sk.AtomicStructure(s.box, s.numbers, s.positions)
+    pot = sk.Potential(st, n, n, slice_thickness=1.9525)
+    probe = sk.Probe(sk.ElectronBeam(200e3), pot.grid, sk.Aperture(20.0))
+    scan = sk.GridScan((1.0, 1.0), (4.0, 4.0), 3, 3)
+    dets = [sk.AnnularDetector(0, 20), sk.AnnularDetector(40, 120), sk.CenterOfMassDetector("cutoff", "mrad")]
+    out = {}
+    for composite in (True, False):
+        opts = sk.ExecutionOptions(form="fused", composite=composite, col_tile=col_tile)
+        out[composite] = sk.STEM.scan(probe, [pot], scan, dets, options=opts, engine=engine)
+    op = O.Potential.from_structure(s, n, n, slice_thickness=1.9525)
+    ores = O.stem_scan(O.ProbeSpec(200e3, 20.0), [(op.grid, op.build(), op.thicknesses)], scan.positions,
+                       [O.DetectorSpec("annular", {"inner": 0, "outer": 20}),
+                        O.DetectorSpec("annular", {"inner": 40, "outer": 120}),
+                        O.DetectorSpec("com", {"mode": "cutoff", "units": "mrad"})])
+    for (a, b, r), (to, te) in zip(zip(out[True], out[False], ores), [(1e-4, 5e-6), (1e-4, 5e-6), (1e-3, 1e-4)]):
+        e_o, e_e = O.rel_l2(a.values, r.ravel()), O.rel_l2(a.values, b.values)
+        print(f"{n}^2 tile {col_tile}: composite vs float64 {e_o:.2e}, vs shared-memory engine {e_e:.2e}")
+        assert e_o <= to and e_e <= te
