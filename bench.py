@@ -515,6 +515,7 @@ def run_jobs(args, sk, L, engine, stream, torch, local):
     jobs = random_jobs(256, seed=1)
     chunk = args.jobs_chunk
     t_table, t_seq, done_table, dur_seq, steps, t_setup = 0.0, 0.0, [], [], 0, 0.0
+    last_table = None
     for c0 in range(0, len(jobs), chunk):
         part = jobs[c0:c0 + chunk]
         table = sk.JobTable()
@@ -540,6 +541,7 @@ def run_jobs(args, sk, L, engine, stream, torch, local):
         _, done = table.run(options=fused, engine=engine)
         t_table += time.perf_counter() - t0
         done_table += list(done)
+        last_table = engine.last_table()  # one graph launch per table call: its kernels and shapes
         plain = sk.ExecutionOptions(form="plain")
         table.run(options=plain, engine=engine)
         torch.cuda.synchronize()
@@ -559,6 +561,7 @@ def run_jobs(args, sk, L, engine, stream, torch, local):
                      "sequential_plain_steps_per_s": steps / t_seq,
                      "table_completion_ms": {"p50": pct(done_table, 50), "p99": pct(done_table, 99)},
                      "sequential_job_ms": {"p50": pct(dur_seq, 50), "p99": pct(dur_seq, 99)},
+                     "last_table_launch": last_table,
                      "timing": "wall clock around each call (synchronising); completion times on the device from "
                                "the start of the call; sequential job times = gaps between completions"},
             "roofline": None, "cpu_baseline": None, "clocks": None, "gpu_launches": None}

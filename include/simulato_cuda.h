@@ -72,6 +72,11 @@ extern "C" {
  * register engine (each line as 3 or 5 register-resident power-of-two transforms of its decimated sub-lines); 0 = the
  * shared-memory Stockham engine. */
 #define SIMK_OPT_COMPOSITE 15
+/* read-only, the last fused simk_job_table_run: host launch calls that ran its slice steps (1: one CUDA graph launch,
+ * with SIMK_OPT_GRAPHS on and SIMK_OPT_TIMING off), the kernels inside them, and the grid shapes they covered */
+#define SIMK_OPT_TABLE_LAUNCHES 16
+#define SIMK_OPT_TABLE_KERNELS 17
+#define SIMK_OPT_TABLE_SHAPES 18
 
 /* ---- Lobato pi choice (LobatoParameterization.PiConstant, LobatoParameterization.swift:15-24) ---- */
 #define SIMK_PI_EXACT 0
@@ -330,8 +335,12 @@ int simk_integrate_gradient_device(simk_context* ctx, int32_t nx, int32_t ny, do
  * (incident = SIMK_JOB_PLANE_WAVE, ones) or a probe (SIMK_JOB_PROBE: aperture, aberrations and tilt from `probe`, its
  * energy replaced by the job's) at (x, y) [A] through its own potential at its own energy; `intensity` (host,
  * nx x ny float64 of that potential's grid) receives |exit wave|^2 after the last slice. Jobs of one grid shape advance
- * together, one row and one column launch per slice step over the jobs still running; with SIMK_FORM_PLAIN they run
- * one after another through the plain path (the sequential baseline). done_ms (optional, n_jobs) receives each job's
+ * together, one row and one column pass per slice step over the jobs still running, each shape on its own stream;
+ * with SIMK_OPT_GRAPHS on (and SIMK_OPT_TIMING off) that whole schedule is captured as one CUDA graph and run by one
+ * launch (SIMK_OPT_TABLE_LAUNCHES / _KERNELS / _SHAPES report it); the context keeps the last such graph with its
+ * device buffers, and a call with the same jobs (potentials, energies, incident waves, positions, settings) only
+ * recomputes the incident waves and launches it again. Turning SIMK_OPT_GRAPHS off releases it. With SIMK_FORM_PLAIN they run one after another
+ * through the plain path (the sequential baseline). done_ms (optional, n_jobs) receives each job's
  * completion time on the device from the start of the call. A potential may serve several jobs of one energy. */
 #define SIMK_JOB_PLANE_WAVE 0
 #define SIMK_JOB_PROBE 1

@@ -208,6 +208,9 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_EPILOGUE_DETECT: *value = c.epilogue_detect; break;
             case SIMK_OPT_POISSON_STREAM: *value = c.poisson_stream; break;
             case SIMK_OPT_COMPOSITE: *value = c.composite; break;
+            case SIMK_OPT_TABLE_LAUNCHES: *value = c.table_launches; break;
+            case SIMK_OPT_TABLE_KERNELS: *value = c.table_kernels; break;
+            case SIMK_OPT_TABLE_SHAPES: *value = c.table_shapes; break;
             case SIMK_OPT_TUNED_COL_TILE: *value = c.last_tuned.col_tile; break;
             case SIMK_OPT_TUNED_TMA: *value = c.last_tuned.tma; break;
             case SIMK_OPT_TUNED_BATCH: *value = c.last_tuned.batch; break;

@@ -152,6 +152,13 @@ struct Context {
     int epilogue_detect = 1;  // channel detectors summed in the last column pass (TMA passes)
     int poisson_stream = 0;   // Poisson noise: 0 = a generator per value and sample, 1 = the reference's one stream
     int composite = 1;        // fused passes at 3 or 5 times a power of two: the composite register engine
+    // the last fused job table: host launch calls for its slice steps (1 when captured as one graph), the kernels in
+    // them, and the grid shapes they covered
+    long long table_launches = 0, table_kernels = 0;
+    int table_shapes = 0;
+    // the last fused job table captured as a graph (its buffers, graph and events), kept for a repeat of the same jobs
+    std::shared_ptr<void> table_cache;
+    std::string table_cache_key;
     int autotune = 0;       // time the launch configurations on first use of a (grid, form)
     struct Tuned {
         int col_tile = -1, tma = -1;
@@ -194,6 +201,8 @@ struct Context {
             if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
         slice_graphs.clear();
         slice_seen.clear();
+        table_cache.reset();
+        table_cache_key.clear();
     }
     ~Context() { drop_graphs(); }
 

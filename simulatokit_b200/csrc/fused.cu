@@ -1915,6 +1915,62 @@ struct StreamsScope {
     }
 };
 
+// A job table's capture: on exit by an exception during the capture the capture is ended and its graph dropped, so the
+// streams can be drained; the instantiated graph is destroyed with it.
+struct TableGraph {
+    cudaStream_t origin = nullptr;
+    bool capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~TableGraph() {
+        if (capturing) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(origin, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();  // an invalidated capture leaves its error behind
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+// The last fused job table captured as a graph, kept in the context for a call with the same jobs: its groups'
+// buffers and tables, the instantiated graph and the events its nodes record. A repeat then computes the incident
+// waves into the same buffers and launches the graph again, without capturing or instantiating it.
+struct TableCache {
+    std::vector<GroupRun> runs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> events;
+    std::vector<std::pair<int, int>> event_jobs;
+    std::vector<int> order;
+    long long kernels = 0;
+    ~TableCache() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto e : events) cudaEventDestroy(e);
+    }
+};
+
+// Everything the captured schedule depends on: the settings that choose its kernels, and per job the potential (its
+// address, transmissions, grid, slice thicknesses), energy, incident wave and position.
+std::string table_key(const Context& ctx, const std::vector<JobSpec>& jobs) {
+    std::string k;
+    auto add = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    const int opts[] = {ctx.form, ctx.tma, ctx.col_tile, ctx.composite, ctx.tcgen05};
+    add(opts, sizeof(opts));
+    for (const JobSpec& j : jobs) {
+        const void* ids[] = {j.pot, j.pot->t.ptr};
+        add(ids, sizeof(ids));
+        const double geo[] = {(double)j.pot->g.nx, (double)j.pot->g.ny, j.pot->g.ex, j.pot->g.ey, j.energy,
+                              j.probe ? 1.0 : 0.0, j.x, j.y};
+        add(geo, sizeof(geo));
+        add(j.pot->dz.data(), j.pot->dz.size() * sizeof(double));
+        if (j.probe) add(&j.probe_spec, sizeof(j.probe_spec));
+    }
+    return k;
+}
+
 // Resets the context's wave table when a job run ends, also by an exception.
 struct WaveTableScope {
     Context& c;
@@ -1942,6 +1998,44 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
         energy_of[j.pot] = j.energy;
     }
     for (auto& kv : energy_of) prepare_transmissions(ctx, *const_cast<PotentialImpl*>(kv.first), kv.second);
+    const bool capture = ctx.form != SIMK_FORM_PLAIN && ctx.graphs && !ctx.timing;
+    const std::string key = capture ? table_key(ctx, jobs) : std::string();
+    if (capture && ctx.table_cache && ctx.table_cache_key == key) {
+        // the same jobs again: their incident waves into the kept buffers, and one launch of the kept graph
+        TableCache& tc = *static_cast<TableCache*>(ctx.table_cache.get());
+        cudaEvent_t start;
+        SIMK_CUDA(cudaEventCreate(&start));
+        try {
+            SIMK_CUDA(cudaEventRecord(start, ctx.stream));
+            for (auto& gr : tc.runs)
+                for (int w = 0; w < gr.G; ++w)
+                    incident_wave(ctx, jobs[gr.ids[w]], gr.waves.as<float2>() + (long long)w * gr.N);
+            SIMK_CUDA(cudaGraphLaunch(tc.exec, ctx.stream));
+            for (auto& gr : tc.runs)
+                for (int w = 0; w < gr.G; ++w)
+                    SIMK_CUDA(cudaMemcpyAsync(jobs[gr.ids[w]].intensity, gr.inten.as<double>() + (long long)w * gr.N,
+                                              gr.N * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+            SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
+            check_device_error(ctx);
+            for (size_t k = 0; k < tc.events.size(); ++k) {
+                float ms = 0;
+                SIMK_CUDA(cudaEventElapsedTime(&ms, start, tc.events[k]));
+                if (done_ms)
+                    for (int q = tc.event_jobs[k].first; q < tc.event_jobs[k].second; ++q) done_ms[tc.order[q]] = ms;
+            }
+        } catch (...) {
+            cudaStreamSynchronize(ctx.stream);
+            cudaEventDestroy(start);
+            throw;
+        }
+        cudaEventDestroy(start);
+        ctx.table_launches = 1;
+        ctx.table_kernels = tc.kernels;
+        ctx.table_shapes = (int)tc.runs.size();
+        return;
+    }
+    ctx.table_cache.reset();  // another table: the kept one's buffers go before this one's are allocated
+    ctx.table_cache_key.clear();
     // the groups: jobs of one grid shape, longest first
     std::map<std::pair<int, int>, std::vector<int>> groups;
     for (int i = 0; i < n; ++i) groups[{jobs[i].pot->g.nx, jobs[i].pot->g.ny}].push_back(i);
@@ -1961,6 +2055,14 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
     WaveTableScope scope{ctx};
     std::vector<GroupRun> runs;  // the fused form's groups, set up first, then advanced side by side
     runs.reserve(groups.size());
+    cudaGraph_t table_graph = nullptr;  // the captured schedule, until the context keeps it
+    cudaGraphExec_t table_exec = nullptr;
+    auto drop_graph = [&] {
+        if (table_exec) cudaGraphExecDestroy(table_exec);
+        if (table_graph) cudaGraphDestroy(table_graph);
+        table_exec = nullptr;
+        table_graph = nullptr;
+    };
     try {
         for (auto& kv : groups) {
             const std::vector<int>& ids = kv.second;
@@ -2040,21 +2142,36 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
             SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the host tables above are freed on return
         }
         // The groups' slice steps, each group on its own stream so that the shapes run side by side (the launches of a
-        // step depend only on the same group's previous step): step s of every group still running, in turn.
+        // step depend only on the same group's previous step): step s of every group still running, in turn. With
+        // SIMK_OPT_GRAPHS (and no per-kernel timing) the whole schedule, every shape and step, the finishing row
+        // passes and the intensities, is captured as one CUDA graph and run by one launch.
         if (!runs.empty()) {
             cudaStream_t home = ctx.stream;
             StreamsScope streams{ctx, home};
-            cudaEvent_t go;
-            SIMK_CUDA(cudaEventCreateWithFlags(&go, cudaEventDisableTiming));
-            streams.events.push_back(go);
-            SIMK_CUDA(cudaEventRecord(go, home));
             for (auto& gr : runs) {
                 cudaStream_t st;
                 SIMK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
                 streams.streams.push_back(st);
-                SIMK_CUDA(cudaStreamWaitEvent(st, go, 0));
                 gr.stream = st;
             }
+            // what the launches create on first use exists before a capture: the plans and the error flag
+            for (auto& gr : runs) {
+                reg_plan(ctx, gr.nx);
+                reg_plan(ctx, gr.ny);
+            }
+            ensure_err_flag(ctx);
+            TableGraph tg;
+            tg.origin = home;
+            if (capture) {
+                SIMK_CUDA(cudaStreamBeginCapture(home, cudaStreamCaptureModeRelaxed));
+                tg.capturing = true;
+            }
+            const long long launches0 = ctx.launches;
+            cudaEvent_t go;
+            SIMK_CUDA(cudaEventCreateWithFlags(&go, cudaEventDisableTiming));
+            streams.events.push_back(go);
+            SIMK_CUDA(cudaEventRecord(go, home));
+            for (auto& gr : runs) SIMK_CUDA(cudaStreamWaitEvent(gr.stream, go, 0));
             int max_s = 0;
             for (auto& gr : runs) max_s = std::max(max_s, gr.S);
             for (int s = 0; s < max_s; ++s) {
@@ -2095,17 +2212,41 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
                     ++ctx.launches;
                     cudaEvent_t e;
                     SIMK_CUDA(cudaEventCreate(&e));
-                    SIMK_CUDA(cudaEventRecord(e, ctx.stream));
+                    // inside a capture an external record becomes a node of the graph that records the event
+                    SIMK_CUDA(cudaEventRecordWithFlags(e, ctx.stream, capture ? cudaEventRecordExternal : 0));
                     events.push_back(e);
                     event_jobs.push_back({gr.first_in_order + A1, gr.first_in_order + A});
                 }
             }
+            ctx.stream = home;
+            for (auto& gr : runs) {  // every group's stream joins the origin stream
+                cudaEvent_t j;
+                SIMK_CUDA(cudaEventCreateWithFlags(&j, cudaEventDisableTiming));
+                streams.events.push_back(j);
+                SIMK_CUDA(cudaEventRecord(j, gr.stream));
+                SIMK_CUDA(cudaStreamWaitEvent(home, j, 0));
+            }
+            ctx.table_kernels = ctx.launches - launches0;
+            ctx.table_shapes = (int)runs.size();
+            if (capture) {
+                tg.capturing = false;
+                SIMK_CUDA(cudaStreamEndCapture(home, &tg.graph));
+                SIMK_CUDA(cudaGraphInstantiate(&tg.exec, tg.graph, 0));
+                SIMK_CUDA(cudaGraphLaunch(tg.exec, home));
+                ctx.table_launches = 1;
+                table_graph = tg.graph;  // from here on owned by this call (then by the context's cache)
+                table_exec = tg.exec;
+                tg.graph = nullptr;
+                tg.exec = nullptr;
+            } else {
+                ctx.table_launches = ctx.table_kernels;
+            }
             for (auto& gr : runs) {
                 for (int w = 0; w < gr.G; ++w)
                     SIMK_CUDA(cudaMemcpyAsync(jobs[gr.ids[w]].intensity, gr.inten.as<double>() + (long long)w * gr.N,
-                                              gr.N * sizeof(double), cudaMemcpyDeviceToHost, gr.stream));
+                                              gr.N * sizeof(double), cudaMemcpyDeviceToHost, home));
             }
-            for (auto& gr : runs) SIMK_CUDA(cudaStreamSynchronize(gr.stream));
+            SIMK_CUDA(cudaStreamSynchronize(home));
         }
         SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
         check_device_error(ctx);
@@ -2115,7 +2256,24 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
             if (done_ms)
                 for (int q = event_jobs[k].first; q < event_jobs[k].second; ++q) done_ms[order[q]] = ms;
         }
+        if (table_exec) {
+            // kept for a call with the same jobs: the groups' buffers, the graph and the events its nodes record
+            auto tc = std::make_shared<TableCache>();
+            tc->runs = std::move(runs);
+            tc->graph = table_graph;
+            tc->exec = table_exec;
+            tc->events = std::move(events);
+            tc->event_jobs = std::move(event_jobs);
+            tc->order = std::move(order);
+            tc->kernels = ctx.table_kernels;
+            events.clear();
+            table_graph = nullptr;
+            table_exec = nullptr;
+            ctx.table_cache = std::static_pointer_cast<void>(tc);
+            ctx.table_cache_key = key;
+        }
     } catch (...) {
+        drop_graph();
         cudaStreamSynchronize(ctx.stream);
         for (auto e : events) cudaEventDestroy(e);
         cudaEventDestroy(start);

@@ -113,6 +113,17 @@ class Engine:
             out[k] = int(v.value)
         return out
 
+    def last_table(self) -> dict:
+        """The last fused job table: host launch calls for its slice steps (1 when captured as one CUDA graph), the
+        kernels inside them and the grid shapes they covered."""
+        out = {}
+        for k, opt in (("launches", L.OPT_TABLE_LAUNCHES), ("kernels", L.OPT_TABLE_KERNELS),
+                       ("shapes", L.OPT_TABLE_SHAPES)):
+            v = C.c_int64(0)
+            L.check(self.lib.simk_context_get_option(self.handle, opt, C.byref(v)))
+            out[k] = int(v.value)
+        return out
+
     def graphs_cached(self) -> int:
         """Slice loops the context holds as instantiated CUDA graphs."""
         v = C.c_int64(0)

@@ -72,6 +72,27 @@ def test_job_table_matches_oracle(engine, table, form):
                     assert done[a] >= done[b]
 
 
+def test_job_table_is_one_launch_over_four_shapes(engine, table):
+    """With CUDA graphs on, the fused table's whole schedule (four grid shapes: 256, 384, 500, 640; every slice step,
+    the finishing row passes and the intensities) runs as one graph launch, and gives the same intensities bit for bit
+    as the same schedule launched kernel by kernel, with completion times in the same order."""
+    t, refs = table
+    outs_g, done_g = t.run(options=sk.ExecutionOptions(form="fused", graphs=True), engine=engine)
+    lt = engine.last_table()
+    print("one-launch table:", lt)
+    assert lt["launches"] == 1 and lt["shapes"] == 4 and lt["kernels"] >= 4
+    outs_e, done_e = t.run(options=sk.ExecutionOptions(form="fused", graphs=False), engine=engine)
+    le = engine.last_table()
+    assert le["launches"] == le["kernels"] == lt["kernels"] and le["shapes"] == 4
+    for a, b in zip(outs_g, outs_e):
+        assert np.array_equal(a, b)
+    assert np.all(done_g > 0)
+    for a in range(len(JOBS)):
+        for b in range(len(JOBS)):
+            if JOBS[a][2] == JOBS[b][2] and refs[a][1] > refs[b][1]:
+                assert done_g[a] >= done_g[b]
+
+
 def test_job_table_refusals(engine):
     s = O.srtio3_cell().repeated(2, 2, 1)
     pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), 256, 256, slice_thickness=1.9525)
