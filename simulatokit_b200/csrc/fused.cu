@@ -520,12 +520,14 @@ constexpr int tma_box_rows(int n) {
         if (n % h == 0) return h;
     return 1;
 }
-// Rows per tile of the row pass: the largest power of two with RB N / 8 <= 256 threads.
-constexpr int rows_per_tile(int n) {
+// Rows per tile of the row pass: the largest power of two with RB N / 8 <= max_threads (256; 384 for the composite
+// engine, whose row blocks then match its two 384-thread column blocks an SM).
+constexpr int rows_per_tile(int n, int max_threads = 256) {
     int r = 1;
-    while (2 * r * (n / 8) <= 256) r *= 2;
+    while (2 * r * (n / 8) <= max_threads) r *= 2;
     return r;
 }
+constexpr int rows_tile(int n, int eng) { return rows_per_tile(n, eng == 4 ? 384 : 256); }
 
 // State an engine keeps per thread: register twiddles (0), the DFT-16 fragments (1), nothing (2), the tcgen05 block
 // state (3), the sub-lines' register twiddles (4).
@@ -785,7 +787,9 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
 }
 
 // rows: tile = RB consecutive rows of one wave (nx % RB == 0); a stage holds those RB rows and the RB rows of t.
-template <int N, int RB, int ENG>
+// IFW >= 0 fixes the transforms at compile time (bit 0: inverse, bit 1: forward; the composite engine's instantiations,
+// so that each holds only its own path's registers); -1 takes inv and fwd as given.
+template <int N, int RB, int ENG, int IFW = -1>
 __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)) fused_rows_tma(float2* __restrict__ psi,
                                                                const float2* __restrict__ tmul,
                                                                const float2* __restrict__ tw, int nx, int nrows,
@@ -793,6 +797,10 @@ __global__ void __launch_bounds__(RB * (N / 8), tc_min_blocks(RB * (N / 8), ENG)
                                                                const float2* const* __restrict__ t_of_wave,
                                                                int tc5_stack) {
     extern __shared__ __align__(128) unsigned char smem_rtma[];
+    if constexpr (IFW >= 0) {
+        inv = IFW & 1;
+        fwd = (IFW >> 1) & 1;
+    }
     constexpr int T = N / 8;
     constexpr int TILE = N * RB;
     __shared__ __align__(8) uint64_t full[2];
@@ -1195,17 +1203,17 @@ inline int pass_blocks_per_sm(int occupancy, int eng, int mb, bool stack) {
     return occupancy;
 }
 
-template <int N, int ENG>
-bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
-                     int fwd, float scale) {
+template <int N, int ENG, int IFW = -1>
+bool launch_rows_tma_k(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows,
+                       int inv, int fwd, float scale) {
     constexpr int T = N / 8;
-    constexpr int RB = rows_per_tile(N);
+    constexpr int RB = rows_tile(N, ENG);
     if constexpr (ENG == 3 && !tc5_tile(N, RB)) {
         return false;
     } else {
     if (nx % RB || nrows % RB || nrows >= (1LL << 31)) return false;
     const size_t smem = tma_pass_smem(N, RB, ENG);
-    auto kern = fused_rows_tma<N, RB, ENG>;
+    auto kern = fused_rows_tma<N, RB, ENG, IFW>;
     static int occupancy = -1;
     if (occupancy < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1224,6 +1232,22 @@ bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* 
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
+    }
+}
+
+// The composite engine's row pass is instantiated per (inverse, forward) pair; the other engines take them at run time.
+template <int N, int ENG>
+bool launch_rows_tma(Context& ctx, const RegPlan& p, float2* psi, const float2* tmul, int nx, long long nrows, int inv,
+                     int fwd, float scale) {
+    if constexpr (ENG == 4) {
+        switch ((inv ? 1 : 0) | (fwd ? 2 : 0)) {
+            case 0: return launch_rows_tma_k<N, ENG, 0>(ctx, p, psi, tmul, nx, nrows, 0, 0, scale);
+            case 1: return launch_rows_tma_k<N, ENG, 1>(ctx, p, psi, tmul, nx, nrows, 1, 0, scale);
+            case 2: return launch_rows_tma_k<N, ENG, 2>(ctx, p, psi, tmul, nx, nrows, 0, 1, scale);
+            default: return launch_rows_tma_k<N, ENG, 3>(ctx, p, psi, tmul, nx, nrows, 1, 1, scale);
+        }
+    } else {
+        return launch_rows_tma_k<N, ENG>(ctx, p, psi, tmul, nx, nrows, inv, fwd, scale);
     }
 }
 
