@@ -53,6 +53,10 @@ extern "C" {
 #define SIMK_OPT_TUNED_COL_TILE 9 /* read-only: the last tuning's choice (-1 before any) */
 #define SIMK_OPT_TUNED_TMA 10
 #define SIMK_OPT_TUNED_BATCH 11
+/* read-only: the last tuning's line-FFT engine where the grid offers a choice (-1: none): the SIMK_OPT_COMPOSITE value
+ * (fused form at lengths 3 or 5 times a power of two) or the SIMK_OPT_TCGEN05 value (bf16x3 form at 256 and 512); the
+ * tuned scan runs with it */
+#define SIMK_OPT_TUNED_ENGINE 19
 /* The bf16x3 form's radix-16 DFT stages on the fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
  * memory) for grid sides 256 and 512, with the data split in three BF16 terms: 2 (default) = six products of N = 96,
  * 64 and 32 per block of 128 vectors (the B terms stacked) into three accumulator blocks, hi x hi alone in one, which

@@ -214,6 +214,7 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_TUNED_COL_TILE: *value = c.last_tuned.col_tile; break;
             case SIMK_OPT_TUNED_TMA: *value = c.last_tuned.tma; break;
             case SIMK_OPT_TUNED_BATCH: *value = c.last_tuned.batch; break;
+            case SIMK_OPT_TUNED_ENGINE: *value = c.last_tuned.engine; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });

@@ -163,6 +163,9 @@ struct Context {
     struct Tuned {
         int col_tile = -1, tma = -1;
         long long batch = -1;
+        // the line-FFT engine (radix plan) where there is a choice: the composite option at lengths 3 or 5 times a
+        // power of two (fused form), the tcgen05 option at 256 and 512 (bf16x3 form); -1 where there is none
+        int engine = -1;
     };
     std::map<std::string, Tuned> tuned;
     Tuned last_tuned;

@@ -174,18 +174,25 @@ void scan_device(Context& ctx, const simk_probe& probe, const std::vector<Potent
         Context& c;
         int tc, tma;
         long long batch;
+        int composite, tcgen05;
         ~Restore() {
             c.col_tile = tc;
             c.tma = tma;
             c.batch = batch;
+            c.composite = composite;
+            c.tcgen05 = tcgen05;
         }
-    } restore{ctx, ctx.col_tile, ctx.tma, ctx.batch};
+    } restore{ctx, ctx.col_tile, ctx.tma, ctx.batch, ctx.composite, ctx.tcgen05};
     if (ctx.autotune && ctx.form != SIMK_FORM_PLAIN && fused_supported(ctx, g)) {
         prepare_transmissions(ctx, *pots[0], probe.energy);
         const Context::Tuned t = autotune(ctx, *pots[0], probe.energy, probe.tilt_x, probe.tilt_y, n_pos);
         if (ctx.col_tile == 0) ctx.col_tile = t.col_tile;
         if (ctx.tma) ctx.tma = t.tma;
         if (ctx.batch == 0) ctx.batch = t.batch;
+        if (t.engine >= 0) {  // the tuned engine (radix plan) for this scan
+            if (ctx.form == SIMK_FORM_FUSED) ctx.composite = t.engine;
+            else ctx.tcgen05 = t.engine;
+        }
     }
     const long long B = batch_size(ctx, g, n_pos);
     ctx.work_a.ensure(B * N * sizeof(float2));

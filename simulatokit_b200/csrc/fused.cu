@@ -1793,7 +1793,20 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
     DeviceBuffer buf((size_t)cap * N * sizeof(float2));
     SIMK_CUDA(cudaMemsetAsync(buf.ptr, 0, (size_t)cap * N * sizeof(float2), ctx.stream));
     const int save_tc = ctx.col_tile, save_tma = ctx.tma, save_timing = ctx.timing;
+    const int save_comp = ctx.composite, save_tc5 = ctx.tcgen05;
     ctx.timing = 0;
+    // the engines to choose from: the composite register engine or the shared-memory one (fused form, lengths 3 or 5
+    // times a power of two), the tcgen05 engine's two product orders or the mma.sync engine (bf16x3 form, 256, 512)
+    std::vector<int> engines{-1};
+    const bool comp_side = comp_length(g.nx) || comp_length(g.ny);
+    const bool tc5_side = (g.nx == 256 || g.nx == 512) && (g.ny == 256 || g.ny == 512);
+    if (ctx.form == SIMK_FORM_FUSED && comp_side) engines = {1, 0};
+    if (ctx.form == SIMK_FORM_BF16X3 && tc5_side) engines = {2, 1, 0};
+    auto set_engine = [&](int e) {
+        if (e < 0) return;
+        if (ctx.form == SIMK_FORM_FUSED) ctx.composite = e;
+        else ctx.tcgen05 = e;
+    };
     cudaEvent_t e0, e1;
     SIMK_CUDA(cudaEventCreate(&e0));
     SIMK_CUDA(cudaEventCreate(&e1));
@@ -1821,24 +1834,30 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
     double best_t = 1e300;
     try {
         const long long b0 = std::min(cap, 256LL);
-        for (int tma : {1, 0}) {
-            if (tma && !save_tma) continue;
-            if (!tma && ctx.form == SIMK_FORM_BF16X3) continue;  // the tensor-core form runs on the TMA passes only
-            for (int tc : {2, 4, 8}) {
-                if (g.ny % tc || tc * (g.nx / 8) > 1024) continue;
-                ctx.tma = tma;
-                ctx.col_tile = tc;
-                const double t = time_per_wave(b0);
-                if (t < best_t) {
-                    best_t = t;
-                    best.col_tile = tc;
-                    best.tma = tma;
-                    best.batch = b0;
+        for (int eng : engines) {
+            set_engine(eng);
+            for (int tma : {1, 0}) {
+                if (tma && !save_tma) continue;
+                if (!tma && ctx.form == SIMK_FORM_BF16X3) continue;  // the tensor-core form runs on the TMA passes only
+                if (!tma && eng == 0 && ctx.form == SIMK_FORM_FUSED) continue;  // the engines differ on TMA passes only
+                for (int tc : {2, 4, 8}) {
+                    if (g.ny % tc || tc * (g.nx / 8) > 1024) continue;
+                    ctx.tma = tma;
+                    ctx.col_tile = tc;
+                    const double t = time_per_wave(b0);
+                    if (t < best_t) {
+                        best_t = t;
+                        best.col_tile = tc;
+                        best.tma = tma;
+                        best.batch = b0;
+                        best.engine = eng;
+                    }
                 }
             }
         }
         ctx.tma = best.tma;
         ctx.col_tile = best.col_tile;
+        set_engine(best.engine);
         // batch: the largest whose time per wave is within 2 % of the fastest, since the per-batch work that is not
         // timed here (probe generation, detection, launches) favours large batches
         std::vector<std::pair<long long, double>> bt{{best.batch, best_t}};
@@ -1854,6 +1873,8 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
         ctx.col_tile = save_tc;
         ctx.tma = save_tma;
         ctx.timing = save_timing;
+        ctx.composite = save_comp;
+        ctx.tcgen05 = save_tc5;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         throw;
@@ -1861,6 +1882,8 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
     ctx.col_tile = save_tc;
     ctx.tma = save_tma;
     ctx.timing = save_timing;
+    ctx.composite = save_comp;
+    ctx.tcgen05 = save_tc5;
     SIMK_CUDA(cudaEventDestroy(e0));
     SIMK_CUDA(cudaEventDestroy(e1));
     SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the scratch batch is freed on return

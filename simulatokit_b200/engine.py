@@ -105,9 +105,11 @@ class Engine:
         return int(v.value)
 
     def tuned(self) -> dict:
-        """The last autotuning's choice (-1 before any): column tile, TMA passes, batch."""
+        """The last autotuning's choice (-1 before any): column tile, TMA passes, batch, and the line-FFT engine where
+        the grid offers one (the composite option of the fused form, the tcgen05 option of bf16x3; -1: none)."""
         out = {}
-        for k, opt in (("col_tile", L.OPT_TUNED_COL_TILE), ("tma", L.OPT_TUNED_TMA), ("batch", L.OPT_TUNED_BATCH)):
+        for k, opt in (("col_tile", L.OPT_TUNED_COL_TILE), ("tma", L.OPT_TUNED_TMA), ("batch", L.OPT_TUNED_BATCH),
+                       ("engine", L.OPT_TUNED_ENGINE)):
             v = C.c_int64(0)
             L.check(self.lib.simk_context_get_option(self.handle, opt, C.byref(v)))
             out[k] = int(v.value)
