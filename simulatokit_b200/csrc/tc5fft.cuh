@@ -115,16 +115,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 __device__ __forceinline__ uint32_t tc5_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
 
 // (re, im) -> three bf16x2 words, re in the low half: hi = bf16(x), lo = bf16(x - hi), lo2 = bf16(x - hi - lo); the
-// differences are exact in float32.
+// differences are exact in float32 and are taken as packed pairs (one sub.f32x2 each, the same bits as two subs).
 __device__ __forceinline__ void tc5_split3(float2 x, uint32_t& h, uint32_t& l, uint32_t& l2) {
     const __nv_bfloat162 hh = __floats2bfloat162_rn(x.x, x.y);
-    const float2 hf = __bfloat1622float2(hh);
-    const float ra = x.x - hf.x, rb = x.y - hf.y;
-    const __nv_bfloat162 ll = __floats2bfloat162_rn(ra, rb);
-    const float2 lf = __bfloat1622float2(ll);
+    const float2 r = psub(x, __bfloat1622float2(hh));
+    const __nv_bfloat162 ll = __floats2bfloat162_rn(r.x, r.y);
+    const float2 r2 = psub(r, __bfloat1622float2(ll));
     h = tc5_bits(hh);
     l = tc5_bits(ll);
-    l2 = tc5_bits(__floats2bfloat162_rn(ra - lf.x, rb - lf.y));
+    l2 = tc5_bits(__floats2bfloat162_rn(r2.x, r2.y));
 }
 
 // Polls of a wait for the tensor core: a stage's products finish within microseconds, so a wait this long means the
@@ -217,7 +216,12 @@ __device__ __forceinline__ void tc5_read(const Tc5& c, uint32_t taddr, float (&d
         tmem_ld16(taddr + 32u, e);
         tmem_ld16(taddr + 64u, f);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) d[i] = (d[i] + e[i]) + f[i];
+        for (int i = 0; i < 16; i += 2) {  // (d + e) + f on (re, im) pairs: add.f32x2, the same bits as scalar adds
+            const float2 s = padd(padd(make_float2(d[i], d[i + 1]), make_float2(e[i], e[i + 1])),
+                                  make_float2(f[i], f[i + 1]));
+            d[i] = s.x;
+            d[i + 1] = s.y;
+        }
     }
 }
 
