@@ -230,6 +230,11 @@ template <int STRIDE> struct SmemCT {
         if constexpr (STRIDE == 0) return base[swz(idx)];
         else return base[swz(idx) * STRIDE];
     }
+    // the slot of an index already swizzled
+    __device__ __forceinline__ float2& slot(int s) const {
+        if constexpr (STRIDE == 0) return base[s];
+        else return base[s * STRIDE];
+    }
 };
 
 // Per-thread twiddles: pass f >= 1 uses w[f - 1][q (R - 1) + r - 1] = W_n^{k r n / (Ns R)}, k = (t + T q) mod Ns.
@@ -297,8 +302,12 @@ __device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const Tw
         }
         if constexpr (SC) {
             line_sync<LT>(bar_id);
+            // swz(t + T i) = (a ^ c_i) + T i with a = t ^ ((t >> 3) mod 16) per thread and c_i = (T / 8) i mod 16 a
+            // constant of the unrolled loop (the carries of t + T i never reach the bits the swizzle flips): each
+            // gather address is one of at most 16 / (T / 8) per-thread bases plus an immediate offset
+            const int a = (int)t ^ (((int)t >> 3) & 15);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = sm.at((int)t + P::T * i);
+            for (int i = 0; i < 8; ++i) v[i] = sm.slot((a ^ (((P::T >> 3) * i) & 15)) + P::T * i);
             line_sync<LT>(bar_id);
         }
         ct_fft_from<N, F + 1, DIR, STRIDE, LT>(v, t, tr, sm, bar_id);
