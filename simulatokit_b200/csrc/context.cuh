@@ -251,6 +251,10 @@ void apply_ctf_device(Context& ctx, const GridGeom& g, double energy, const simk
                       const double* in_re, const double* in_im, double* out_re, double* out_im, double* out_intensity);
 void probe_spectrum_device(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
                            DeviceBuffer* out_f64);
+// The same spectrum into buffers the caller keeps (grown when too small), with no allocation when they are large
+// enough and no synchronisation: for many probes in a row on one stream.
+void probe_spectrum_into(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
+                         DeviceBuffer& tmp, DeviceBuffer& norm);
 void launch_ramps(Context& ctx, const GridGeom& g, const double* positions_dev, long long first, int count,
                   float2* rx, float2* ry);
 void launch_probes(Context& ctx, const GridGeom& g, const float2* spectrum, const float2* rx, const float2* ry,

@@ -1922,8 +1922,16 @@ __global__ void k_intensity(const float2* __restrict__ psi, long long n, double*
 }
 int grid_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 16)); }
 
-// The incident wave of job j into psi (N float2): ones, or the probe IFFT(Psi0 r_x r_y) at (x, y).
-void incident_wave(Context& ctx, const JobSpec& j, float2* psi) {
+// Buffers the incident probes of a job table share, grown to the largest grid once: the jobs' probes are formed one
+// after another on one stream, so no job allocates, frees or waits.
+struct ProbeScratch {
+    DeviceBuffer spectrum, tmp, norm, rx, ry;
+    DeviceBuffer positions;  // (x, y) of every job, uploaded once
+};
+
+// The incident wave of job j (index `job` of the table) into psi (N float2): ones, or the probe IFFT(Psi0 r_x r_y) at
+// (x, y).
+void incident_wave(Context& ctx, const JobSpec& j, int job, ProbeScratch& sc, float2* psi) {
     const GridGeom& g = j.pot->g;
     const long long N = g.count();
     if (!j.probe) {
@@ -1934,14 +1942,37 @@ void incident_wave(Context& ctx, const JobSpec& j, float2* psi) {
     }
     simk_probe pr = j.probe_spec;
     pr.energy = j.energy;
-    DeviceBuffer spectrum, pos(2 * sizeof(double)), rx(g.nx * sizeof(float2)), ry(g.ny * sizeof(float2));
-    probe_spectrum_device(ctx, g, pr, spectrum, nullptr);
-    const double xy[2] = {j.x, j.y};
-    SIMK_CUDA(cudaMemcpyAsync(pos.ptr, xy, sizeof(xy), cudaMemcpyHostToDevice, ctx.stream));
-    launch_ramps(ctx, g, pos.as<double>(), 0, 1, rx.as<float2>(), ry.as<float2>());
-    launch_probes(ctx, g, spectrum.as<float2>(), rx.as<float2>(), ry.as<float2>(), 1, psi, 1.0f);
+    probe_spectrum_into(ctx, g, pr, sc.spectrum, sc.tmp, sc.norm);
+    sc.rx.ensure(g.nx * sizeof(float2));
+    sc.ry.ensure(g.ny * sizeof(float2));
+    launch_ramps(ctx, g, sc.positions.as<double>(), job, 1, sc.rx.as<float2>(), sc.ry.as<float2>());
+    launch_probes(ctx, g, sc.spectrum.as<float2>(), sc.rx.as<float2>(), sc.ry.as<float2>(), 1, psi, 1.0f);
     fft2(ctx.plan(g.ny, 32), ctx.plan(g.nx, 32), psi, g.nx, g.ny, 1, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);
-    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the temporaries above are freed on return
+}
+
+// The scratch for the table's probes: sized for the largest probe grid, and every job's position on the device.
+void probe_scratch(Context& ctx, const std::vector<JobSpec>& jobs, ProbeScratch& sc) {
+    long long n_max = 0;
+    int nx_max = 0, ny_max = 0;
+    std::vector<double> xy(2 * jobs.size());
+    for (size_t i = 0; i < jobs.size(); ++i) {
+        xy[2 * i] = jobs[i].x;
+        xy[2 * i + 1] = jobs[i].y;
+        if (!jobs[i].probe) continue;
+        n_max = std::max(n_max, jobs[i].pot->g.count());
+        nx_max = std::max(nx_max, jobs[i].pot->g.nx);
+        ny_max = std::max(ny_max, jobs[i].pot->g.ny);
+    }
+    if (n_max == 0) return;
+    sc.spectrum.ensure(n_max * sizeof(float2));
+    sc.tmp.ensure(n_max * sizeof(double2));
+    sc.norm.ensure(sizeof(double));
+    sc.rx.ensure(nx_max * sizeof(float2));
+    sc.ry.ensure(ny_max * sizeof(float2));
+    sc.positions.ensure(xy.size() * sizeof(double));
+    SIMK_CUDA(cudaMemcpyAsync(sc.positions.ptr, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    SIMK_CUDA(cudaStreamSynchronize(ctx.stream));  // the host copy of the positions is freed on return
 }
 
 // One grid shape's jobs in a fused job-table run: their waves, intensities, per-step tables and stream.
@@ -2059,13 +2090,15 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
     if (capture && ctx.table_cache && ctx.table_cache_key == key) {
         // the same jobs again: their incident waves into the kept buffers, and one launch of the kept graph
         TableCache& tc = *static_cast<TableCache*>(ctx.table_cache.get());
+        ProbeScratch sc;
+        probe_scratch(ctx, jobs, sc);
         cudaEvent_t start;
         SIMK_CUDA(cudaEventCreate(&start));
         try {
             SIMK_CUDA(cudaEventRecord(start, ctx.stream));
             for (auto& gr : tc.runs)
                 for (int w = 0; w < gr.G; ++w)
-                    incident_wave(ctx, jobs[gr.ids[w]], gr.waves.as<float2>() + (long long)w * gr.N);
+                    incident_wave(ctx, jobs[gr.ids[w]], gr.ids[w], sc, gr.waves.as<float2>() + (long long)w * gr.N);
             SIMK_CUDA(cudaGraphLaunch(tc.exec, ctx.stream));
             for (auto& gr : tc.runs)
                 for (int w = 0; w < gr.G; ++w)
@@ -2102,6 +2135,8 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
     auto tilt = [&](const JobSpec& j, int k) {
         return j.probe ? (k == 0 ? j.probe_spec.tilt_x : j.probe_spec.tilt_y) : 0.0;
     };
+    ProbeScratch probes;  // the incident probes' buffers, kept to the end of the call
+    probe_scratch(ctx, jobs, probes);
     cudaEvent_t start;
     SIMK_CUDA(cudaEventCreate(&start));
     std::vector<cudaEvent_t> events;
@@ -2129,7 +2164,7 @@ void run_job_table(Context& ctx, const std::vector<JobSpec>& jobs, double* done_
             const int S = jobs[ids[0]].pot->n_slices();
             DeviceBuffer waves((size_t)G * N * sizeof(float2)), inten((size_t)G * N * sizeof(double));
             float2* psi = waves.as<float2>();
-            for (int w = 0; w < G; ++w) incident_wave(ctx, jobs[ids[w]], psi + (long long)w * N);
+            for (int w = 0; w < G; ++w) incident_wave(ctx, jobs[ids[w]], ids[w], probes, psi + (long long)w * N);
             const int first_in_order = (int)order.size();
             order.insert(order.end(), ids.begin(), ids.end());
             if (ctx.form == SIMK_FORM_PLAIN) {

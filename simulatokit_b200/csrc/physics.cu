@@ -518,8 +518,10 @@ __global__ void k_scale_d2(double2* a, long long N, const double* norm2) {
         a[i] = make_double2(a[i].x * f, a[i].y * f);
 }
 
-void probe_spectrum_device(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
-                           DeviceBuffer* out_f64) {
+namespace {
+// The normalised probe spectrum in float64 into tmp (N double2, norm one double) and as complex64 into out.
+void probe_spectrum_launch(Context& ctx, const GridGeom& g, const simk_probe& probe, double2* tmp, double* norm,
+                           float2* out) {
     SIMK_REQUIRE(std::isfinite(probe.energy) && probe.energy > 0, "the energy must be finite and positive");
     SIMK_REQUIRE(probe.semiangle_mrad > 0 && !std::isnan(probe.semiangle_mrad), "invalid aperture");
     for (int i = 0; i < 25; ++i) SIMK_REQUIRE(std::isfinite(probe.aberrations[i]), "every aberration must be finite");
@@ -533,14 +535,30 @@ void probe_spectrum_device(Context& ctx, const GridGeom& g, const simk_probe& pr
     p.dax = rsx * 1e3 * p.lambda * 1e-3;
     p.day = rsy * 1e3 * p.lambda * 1e-3;
     for (int i = 0; i < 25; ++i) p.ab[i] = probe.aberrations[i];
-    DeviceBuffer tmp(N * sizeof(double2)), norm(sizeof(double));
-    k_probe_spectrum<<<blocks_for(N), 256, 0, ctx.stream>>>(tmp.as<double2>(), grid_dev(g), p);
-    k_norm2<<<1, 1024, 0, ctx.stream>>>(tmp.as<double2>(), N, norm.as<double>());
-    k_scale_d2<<<blocks_for(N), 256, 0, ctx.stream>>>(tmp.as<double2>(), N, norm.as<double>());
-    out_f32.alloc(N * sizeof(float2));
-    k_to_float2<<<blocks_for(N), 256, 0, ctx.stream>>>(out_f32.as<float2>(), tmp.as<double2>(), N);
+    k_probe_spectrum<<<blocks_for(N), 256, 0, ctx.stream>>>(tmp, grid_dev(g), p);
+    k_norm2<<<1, 1024, 0, ctx.stream>>>(tmp, N, norm);
+    k_scale_d2<<<blocks_for(N), 256, 0, ctx.stream>>>(tmp, N, norm);
+    k_to_float2<<<blocks_for(N), 256, 0, ctx.stream>>>(out, tmp, N);
     ctx.launches += 4;
     SIMK_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void probe_spectrum_into(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
+                         DeviceBuffer& tmp, DeviceBuffer& norm) {
+    const long long N = g.count();
+    tmp.ensure(N * sizeof(double2));
+    norm.ensure(sizeof(double));
+    out_f32.ensure(N * sizeof(float2));
+    probe_spectrum_launch(ctx, g, probe, tmp.as<double2>(), norm.as<double>(), out_f32.as<float2>());
+}
+
+void probe_spectrum_device(Context& ctx, const GridGeom& g, const simk_probe& probe, DeviceBuffer& out_f32,
+                           DeviceBuffer* out_f64) {
+    const long long N = g.count();
+    DeviceBuffer tmp(N * sizeof(double2)), norm(sizeof(double));
+    out_f32.alloc(N * sizeof(float2));
+    probe_spectrum_launch(ctx, g, probe, tmp.as<double2>(), norm.as<double>(), out_f32.as<float2>());
     if (out_f64) {
         out_f64->alloc(N * sizeof(double2));
         SIMK_CUDA(cudaMemcpyAsync(out_f64->ptr, tmp.ptr, N * sizeof(double2), cudaMemcpyDeviceToDevice, ctx.stream));
