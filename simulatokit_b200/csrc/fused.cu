@@ -521,8 +521,10 @@ __device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool n
 }
 
 // columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each.
-// ENG 0: register-resident float32 Cooley-Tukey passes; ENG 1: the tile is transformed in place in shared memory with
-// radix-16 tensor-core stages (tcfft.cuh, the bf16x3 form).
+// Engines: 0 register-resident float32 Cooley-Tukey passes (powers of two); 1 radix-16 stages as mma.sync products of
+// split-BF16 operands on a shared-memory tile (tcfft.cuh, the bf16x3 form); 2 float32 shared-memory Stockham
+// (ccfft.cuh); 3 radix-16 stages as tcgen05.mma products (tc5fft.cuh, the bf16x3 form at 256 and 512); 4 the composite
+// register engine (lengths 3 or 5 times a power of two: R sub-lines of engine 0).
 // Height of the column pass's TMA boxes: the largest divisor of N that is at most 256 (the box limit).
 constexpr int tma_box_rows(int n) {
     for (int h = 256; h > 1; --h)
