@@ -270,12 +270,25 @@ CPU_SAMPLE = ("{n} of 4096 positions x 20 slices per step, C++17 float64 restate
               "(oracle/cpu/simk_cpu.cpp), {threads} threads over positions")
 
 
+def host_threads() -> int:
+    """Every host thread this process may run on."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return max(1, os.cpu_count() or 1)
+
+
+def cpu_sample_size(requested: int, threads: int) -> int:
+    """Positions of the CPU sample: the requested count, at least two per thread so that every thread has work."""
+    return min(4096, max(requested, 2 * threads))
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = min(8, os.cpu_count() or 1)
-    ref = CpuReference(args.cpu_positions, threads)
+    threads = host_threads()  # all the host threads it can use
+    ref = CpuReference(cpu_sample_size(args.cpu_positions, threads), threads)
     for _ in range(args.warmup):
         ref.warm_up()
     vals = []
@@ -927,11 +940,12 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = min(8, os.cpu_count() or 1)
-        v, dt, n, ref_vals = cpu_reference(args.cpu_positions, threads, want_values=True)
+        threads = host_threads()
+        n_cpu = cpu_sample_size(args.cpu_positions, threads)
+        v, dt, n, ref_vals = cpu_reference(n_cpu, threads, want_values=True)
         cpu = {"value": v, "unit": "probe.slice steps/s", "cores": threads, "kind": "port",
                "sample": CPU_SAMPLE.format(n=n, threads=threads) + f" ({dt:.1f} s)"}
-        idx = sample_indices(args.cpu_positions)
+        idx = sample_indices(n_cpu)
         for f, vals in form_values.items():
             errs = [float(np.linalg.norm(vals[d][idx] - ref_vals[d]) / np.linalg.norm(ref_vals[d]))
                     for d in range(len(dets))]
