@@ -76,6 +76,11 @@ extern "C" {
  * register engine (each line as 3 or 5 register-resident power-of-two transforms of its decimated sub-lines); 0 = the
  * shared-memory Stockham engine. */
 #define SIMK_OPT_COMPOSITE 15
+/* The fused form's column passes at grid sides 512 and 256: 1 (default) = tiles of 8 (512) or 16 (256) columns, one
+ * thread transforming the same rows of two adjacent columns, so that every global row segment is 64 or 128 bytes wide
+ * (the pass then moves its bytes at close to the device's copy rate), where SIMK_OPT_COL_TILE is 0 or that width;
+ * 0 = one column a thread, SIMK_OPT_COL_TILE (default 4) columns a tile. */
+#define SIMK_OPT_PAIRED 20
 /* read-only, the last fused simk_job_table_run: host launch calls that ran its slice steps (1: one CUDA graph launch,
  * with SIMK_OPT_GRAPHS on and SIMK_OPT_TIMING off), the kernels inside them, and the grid shapes they covered */
 #define SIMK_OPT_TABLE_LAUNCHES 16

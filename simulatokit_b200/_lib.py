@@ -22,6 +22,7 @@ OPT_GRAPHS_CACHED = 7
 OPT_AUTOTUNE, OPT_TUNED_COL_TILE, OPT_TUNED_TMA, OPT_TUNED_BATCH = 8, 9, 10, 11
 OPT_TCGEN05, OPT_EPILOGUE_DETECT, OPT_POISSON_STREAM, OPT_COMPOSITE = 12, 13, 14, 15
 OPT_TABLE_LAUNCHES, OPT_TABLE_KERNELS, OPT_TABLE_SHAPES, OPT_TUNED_ENGINE = 16, 17, 18, 19
+OPT_PAIRED = 20
 PI_EXACT, PI_ABTEM_FLOAT32 = 0, 1
 DET_ANNULAR, DET_PIXELATED, DET_COM, DET_SEGMENTED, DET_BINNED = 0, 1, 2, 3, 4
 MAXANGLE_CUTOFF, MAXANGLE_VALID, MAXANGLE_FULL = 0, 1, 2

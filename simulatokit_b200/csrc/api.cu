@@ -163,6 +163,7 @@ int simk_context_set_option(simk_context* ctx, int32_t option, int64_t value) {
                 c.poisson_stream = (int)value;
                 break;
             case SIMK_OPT_COMPOSITE: c.composite = value ? 1 : 0; break;
+            case SIMK_OPT_PAIRED: c.paired = value ? 1 : 0; break;
             default: throw Error(SIMK_ERR_INVALID, "unknown option");
         }
     });
@@ -208,6 +209,7 @@ int simk_context_get_option(simk_context* ctx, int32_t option, int64_t* value) {
             case SIMK_OPT_EPILOGUE_DETECT: *value = c.epilogue_detect; break;
             case SIMK_OPT_POISSON_STREAM: *value = c.poisson_stream; break;
             case SIMK_OPT_COMPOSITE: *value = c.composite; break;
+            case SIMK_OPT_PAIRED: *value = c.paired; break;
             case SIMK_OPT_TABLE_LAUNCHES: *value = c.table_launches; break;
             case SIMK_OPT_TABLE_KERNELS: *value = c.table_kernels; break;
             case SIMK_OPT_TABLE_SHAPES: *value = c.table_shapes; break;

@@ -152,6 +152,7 @@ struct Context {
     int epilogue_detect = 1;  // channel detectors summed in the last column pass (TMA passes)
     int poisson_stream = 0;   // Poisson noise: 0 = a generator per value and sample, 1 = the reference's one stream
     int composite = 1;        // fused passes at 3 or 5 times a power of two: the composite register engine
+    int paired = 1;           // fused column passes at 256 and 512 on column pairs (engine 5)
     // the last fused job table: host launch calls for its slice steps (1 when captured as one graph), the kernels in
     // them, and the grid shapes they covered
     long long table_launches = 0, table_kernels = 0;

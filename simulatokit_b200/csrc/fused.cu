@@ -314,6 +314,78 @@ __device__ __forceinline__ void ct_fft_from(float2 (&v)[8], unsigned t, const Tw
     }
 }
 
+// ---- column pairs (engine 5): one thread transforms the same rows of two adjacent columns -----------------------------
+// Thread (c, t) of a column tile eight columns wide holds columns 2c and 2c + 1 of rows t + T i: every load and store of
+// the tile moves both as one 16-byte access, and the exchanges keep the pair together in one float4 slot. Pair c's
+// exchange region is N float4 slots, slot s at swz(s) ^ 2c: a quarter warp (two t, four c) then reaches eight
+// different 16-byte bank groups in every scatter and gather of these plans (bit 0 of the swizzled slot tells the two t
+// apart, 2c the four pairs). The twiddles depend on t only, so both columns share them. `after_first_sync` runs right
+// after the first barrier of the transform (by then every thread has finished what preceded the transform).
+template <int N, int F, int DIR, typename Hook>
+__device__ __forceinline__ void ct2_fft_from(float2 (&v0)[8], float2 (&v1)[8], unsigned t, const TwRegs<N>& tr,
+                                             float4* __restrict__ region, int xc, Hook&& after_first_sync) {
+    using P = Pow2<N>;
+    if constexpr (F < P::NP) {
+        constexpr int R = P::radix(F), NS = P::ns(F), Q = 8 / R;
+        constexpr bool SC = (F + 1 < P::NP);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            float2 a[R], b[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                a[r] = v0[q + r * Q];
+                b[r] = v1[q + r * Q];
+            }
+            if constexpr (F > 0) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const float2 w = tr.w[F - 1][q * (R - 1) + r - 1];
+                    a[r] = (DIR < 0) ? cmul(a[r], w) : cmulc(a[r], w);
+                    b[r] = (DIR < 0) ? cmul(b[r], w) : cmulc(b[r], w);
+                }
+            }
+            if constexpr (R == 2) {
+                bfly2<DIR>(a);
+                bfly2<DIR>(b);
+            } else if constexpr (R == 4) {
+                bfly4<DIR>(a);
+                bfly4<DIR>(b);
+            } else {
+                bfly8<DIR>(a);
+                bfly8<DIR>(b);
+            }
+            if constexpr (SC) {
+                const int jj = (int)t + P::T * q;
+                const int k = jj & (NS - 1);
+                const int o = (jj - k) * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) region[swz(o + r * NS) ^ xc] = make_float4(a[r].x, a[r].y, b[r].x, b[r].y);
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    v0[q + r * Q] = a[r];
+                    v1[q + r * Q] = b[r];
+                }
+            }
+        }
+        if constexpr (SC) {
+            __syncthreads();
+            if constexpr (F == 0) after_first_sync();
+            // as in ct_fft_from: swz(t + T i) ^ xc = (a ^ c_i) + T i with the per-thread a = swz(t) ^ xc (xc < 8 and
+            // swz(t) < T leave T i's bits alone)
+            const int a0 = ((int)t ^ (((int)t >> 3) & 15)) ^ xc;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float4 x = region[(a0 ^ (((P::T >> 3) * i) & 15)) + P::T * i];
+                v0[i] = make_float2(x.x, x.y);
+                v1[i] = make_float2(x.z, x.w);
+            }
+            __syncthreads();
+        }
+        ct2_fft_from<N, F + 1, DIR>(v0, v1, t, tr, region, xc, after_first_sync);
+    }
+}
+
 // ---- composite lengths N = R M (R = 3 or 5, M a power of two >= 64): the register engine on R sub-lines ---------------
 // A line's N / 8 threads form R sub-lines of TS = M / 8 threads; thread (g, u) is sub-line g, thread u. Decimation in
 // frequency from natural order (comp_dif_in, then the M-point register transform of each sub-line):
@@ -540,11 +612,11 @@ constexpr int rows_per_tile(int n, int max_threads = 256) {
 }
 constexpr int rows_tile(int n, int eng) { return rows_per_tile(n, eng == 4 ? 384 : 256); }
 
-// State an engine keeps per thread: register twiddles (0), the DFT-16 fragments (1), nothing (2), the tcgen05 block
+// State an engine keeps per thread: register twiddles (0, 5), the DFT-16 fragments (1), nothing (2), the tcgen05 block
 // state (3), the sub-lines' register twiddles (4).
 template <int N, int ENG>
 using EngineState = std::conditional_t<
-    ENG == 0, TwRegs<N>,
+    ENG == 0 || ENG == 5, TwRegs<N>,
     std::conditional_t<ENG == 1, Dft16Frags,
                        std::conditional_t<ENG == 3, Tc5, std::conditional_t<ENG == 4, TwRegs<CompPlan<N>::M>, int>>>>;
 
@@ -602,11 +674,14 @@ constexpr int tc_min_blocks(int threads, int eng) {
     if (eng == 1 || eng == 3) return threads <= 256 ? 2 : 1;
     if (eng == 0) return threads == 256 ? 3 : 1;
     if (eng == 4) return threads <= 256 ? 3 : (threads <= 384 ? 2 : 1);
+    if (eng == 5) return threads <= 256 ? 2 : 1;
     return 1;
 }
+// Threads across a column tile: one per column, or one per column pair (engine 5).
+constexpr int cols_tx(int tc, int eng) { return eng == 5 ? tc / 2 : tc; }
 
 template <int N, int TC, int MODE, int ENG>
-__global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG))
+__global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols_tx(TC, ENG) * (N / 8), ENG))
     fused_cols_tma(const __grid_constant__ CUtensorMap map,
                                                                const __grid_constant__ CUtensorMap pmap,
                                                                float2* __restrict__ psi, float pscale, int ny,
@@ -618,26 +693,35 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     constexpr int BOXH = tma_box_rows(N);
     constexpr int NBOX = N / BOXH;
     constexpr int TILE = N * TC;  // float2 per tile
-    constexpr uint32_t STAGE_BYTES = 2u * TILE * sizeof(float2);
+    // engine 5: a stage holds only the wave tile and the P tile has one buffer of its own (refilled for the next tile
+    // once the multiply is done), so that two CTAs of eight-column tiles fit an SM
+    constexpr bool PSEP = (ENG == 5);
+    constexpr int TX = cols_tx(TC, ENG);
+    constexpr int SST = (PSEP ? 1 : 2) * TILE;  // float2 per stage
+    constexpr uint32_t STAGE_BYTES = (uint32_t)SST * sizeof(float2);
     __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t pfull;
     __shared__ int abort_flag;
     __shared__ uint32_t tmem_slot;
     __shared__ __align__(8) uint64_t mma_bar;
+    __shared__ double red5[PSEP && MODE == 3 ? TX * T / 32 * 64 : 1];  // engine 5's detector sums (C <= 64)
     float2* stages = reinterpret_cast<float2*>(smem_tma);
+    [[maybe_unused]] float2* const ptile = stages + 2 * SST;  // engine 5's P tile
     const int c = threadIdx.x;
     const unsigned t = threadIdx.y;
-    const int tid = (int)t * TC + c;
+    const int tid = (int)t * TX + c;
     const unsigned tiles_per_wave = (unsigned)(ny / TC);
     const unsigned ntiles = (unsigned)count * tiles_per_wave;  // < 2^31: checked by the launcher
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
+        mbar_init(&pfull, 1);
         fence_barrier_init();
         abort_flag = 0;
     }
     __syncthreads();
     [[maybe_unused]] EngineState<N, ENG> eng;
-    if constexpr (ENG == 0) tw_load<N, 1>(eng, t, tw);
+    if constexpr (ENG == 0 || ENG == 5) tw_load<N, 1>(eng, t, tw);
     else if constexpr (ENG == 4) tw_load<CompPlan<N>::M, 1, CompPlan<N>::R>(eng, t % CompPlan<N>::TS, tw);
     else if constexpr (ENG == 1) eng = dft16_frags(tid & 31);
     else if constexpr (ENG == 3)
@@ -646,21 +730,33 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
     auto issue = [&](unsigned tile, int s) {
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
-        float2* dst = stages + s * 2 * TILE;
+        float2* dst = stages + s * SST;
         const int prow = p_row ? p_row[b] * N : 0;  // job tables: this wave's propagator among the stacked ones
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
 #pragma unroll
         for (int k = 0; k < NBOX; ++k) {
             tma_load_2d(dst + k * BOXH * TC, &map, &full[s], 2 * iy0, b * N + k * BOXH);
-            tma_load_2d(dst + TILE + k * BOXH * TC, &pmap, &full[s], 2 * iy0, prow + k * BOXH);
+            if constexpr (!PSEP) tma_load_2d(dst + TILE + k * BOXH * TC, &pmap, &full[s], 2 * iy0, prow + k * BOXH);
         }
     };
+    // engine 5: the P tile of `tile` into its own buffer, completing on pfull (one phase per tile)
+    [[maybe_unused]] auto issue_p = [&](unsigned tile) {
+        const int b = (int)(tile / tiles_per_wave);
+        const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
+        const int prow = p_row ? p_row[b] * N : 0;
+        mbar_arrive_expect_tx(&pfull, (uint32_t)TILE * sizeof(float2));
+#pragma unroll
+        for (int k = 0; k < NBOX; ++k) tma_load_2d(ptile + k * BOXH * TC, &pmap, &pfull, 2 * iy0, prow + k * BOXH);
+    };
     unsigned tile = blockIdx.x;
-    if (tid == 0 && tile < ntiles) issue(tile, 0);
+    if (tid == 0 && tile < ntiles) {
+        issue(tile, 0);
+        if constexpr (PSEP) issue_p(tile);
+    }
     for (int it = 0; tile < ntiles; tile += gridDim.x, ++it) {
         const int s = it & 1;
-        float2* buf = stages + s * 2 * TILE;
-        const float2* pbuf = buf + TILE;
+        float2* buf = stages + s * SST;
+        const float2* pbuf = PSEP ? ptile : buf + TILE;
         const unsigned next = tile + gridDim.x;
         if (tid == 0) {
             // the previous tile's TMA store must have read its shared-memory source (a stage or the scratch tile)
@@ -670,6 +766,15 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             const bool more = !abort_flag && next < ntiles;
             if (more) issue(next, s ^ 1);
             stage_wait(full, s, it, more, err, &abort_flag);
+            if constexpr (PSEP) {
+                // this tile's P, issued at the start or once the previous tile's multiply was done; waited for after
+                // an abandoned wave copy too, so that no copy is in flight when the block leaves
+                if (!mbar_wait_bounded(&pfull, (uint32_t)(it & 1))) {
+                    atomicExch(err, 1);
+                    if (!abort_flag && more) mbar_wait_bounded(&full[s ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+                    abort_flag = 1;
+                }
+            }
         }
         __syncthreads();
         if (abort_flag) break;
@@ -690,6 +795,39 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             // thread 0 stores the tile with TMA after the barrier below
 #pragma unroll
             for (int i = 0; i < 8; ++i) buf[(t + T * i) * TC + c] = v[i];
+            store_src = buf;
+        } else if constexpr (ENG == 5) {
+            // column pairs: thread (c, t) holds columns 2c, 2c + 1 of rows t + T i (one 16-byte access per row)
+            float4* const tile4 = reinterpret_cast<float4*>(buf);
+            const float4* const p4 = reinterpret_cast<const float4*>(pbuf);
+            float2 v0[8], v1[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float4 x = tile4[(t + T * i) * TX + c];
+                v0[i] = make_float2(x.x, x.y);
+                v1[i] = make_float2(x.z, x.w);
+            }
+            __syncthreads();  // the wave tile has been read: it becomes the pairs' exchange regions
+            static_assert(TX == 4 || TX == 8, "column pairs: four or eight pairs a tile");
+            float4* const region = tile4 + c * N;
+            // the slot XOR that spreads a quarter warp (two t and four pairs, or one t and eight) over the bank groups
+            const int xc = (TX == 4) ? 2 * c : c;
+            ct2_fft_from<N, 0, -1>(v0, v1, t, eng, region, xc, [] {});
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float4 pp = p4[(t + T * i) * TX + c];
+                v0[i] = cmul(v0[i], make_float2(pp.x, pp.y)) * pscale;
+                v1[i] = cmul(v1[i], make_float2(pp.z, pp.w)) * pscale;
+            }
+            if constexpr (MODE == 0) {
+                // behind the inverse transform's first barrier every thread has multiplied: the next tile's P may come
+                ct2_fft_from<N, 0, +1>(v0, v1, t, eng, region, xc, [&] {
+                    if (tid == 0 && !abort_flag && next < ntiles) issue_p(next);
+                });
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                tile4[(t + T * i) * TX + c] = make_float4(v0[i].x, v0[i].y, v1[i].x, v1[i].y);
             store_src = buf;
         } else if constexpr (ENG == 4) {
             // composite length: R sub-lines of TS threads per column; a sub-line's exchanges use its own part of the
@@ -784,11 +922,16 @@ __global__ void __launch_bounds__(TC * (N / 8), tc_min_blocks(TC * (N / 8), ENG)
             for (int k = 0; k < NBOX; ++k) tma_store_2d(&map, store_src + k * BOXH * TC, 2 * iy0, b * N + k * BOXH);
             bulk_commit();
         }
+        if constexpr (PSEP && MODE != 0) {
+            // without an inverse transform the P tile is free from the barrier above on
+            if (tid == 0 && !abort_flag && next < ntiles) issue_p(next);
+        }
         if constexpr (MODE == 3) {
             // the tile the result is not in holds the warps' sums (TILE float2 >= NT / 32 * C doubles, C <= 64): the P
-            // tile (read by now), or for the composite engine, whose result is in the P tile, the wave tile
-            float2* sums = (ENG == 4) ? buf : buf + TILE;
-            detect_tile<TC * T>(store_src, det, b, (iy - c) / TC, tid, reinterpret_cast<double*>(sums));
+            // tile (read by now), or for the composite engine, whose result is in the P tile, the wave tile; engine 5,
+            // whose P buffer is being refilled, has an array of its own
+            double* sums = PSEP ? red5 : reinterpret_cast<double*>((ENG == 4) ? buf : buf + TILE);
+            detect_tile<TX * T>(store_src, det, b, (iy - c) / TC, tid, sums);
             fence_proxy_async_shared();  // the sums were written by this proxy; the next copy into the stage by TMA
             __syncthreads();  // the partials' reads of the tile and of the sums precede the next copy into the stage
         }
@@ -1180,8 +1323,9 @@ void ensure_err_flag(Context& ctx) {
 // Dynamic shared memory of a TMA pass: two stages of (wave tile, t or P tile), plus the shared-memory engines' scratch
 // tile (1, 2) or the tcgen05 engine's operands (3).
 constexpr size_t tma_pass_smem(int n, int lines, int eng) {
-    return eng == 3 ? 4 * (size_t)n * lines * sizeof(float2) + tc5_smem_bytes(tc5_blocks(n, lines))
-                    : (eng != 0 && eng != 4 ? 5 : 4) * (size_t)n * lines * sizeof(float2);
+    return eng == 3   ? 4 * (size_t)n * lines * sizeof(float2) + tc5_smem_bytes(tc5_blocks(n, lines))
+           : eng == 5 ? 3 * (size_t)n * lines * sizeof(float2)  // two wave stages and one P tile
+                      : (eng != 0 && eng != 4 ? 5 : 4) * (size_t)n * lines * sizeof(float2);
 }
 
 // Blocks of `kern` (threads, dynamic shared memory) that fit on one SM by its registers, shared memory, threads and
@@ -1275,8 +1419,8 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     if (occupancy < 0) {
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         SIMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, TC * T, smem));
-        occupancy = std::max(occupancy, fitting_blocks((const void*)kern, TC * T, smem, ctx.device));
+        SIMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, cols_tx(TC, ENG) * T, smem));
+        occupancy = std::max(occupancy, fitting_blocks((const void*)kern, cols_tx(TC, ENG) * T, smem, ctx.device));
     }
     const int stack = ctx.tcgen05 == 2 ? 1 : 0;
     const int blocks_per_sm = pass_blocks_per_sm(occupancy, ENG, ENG == 3 ? tc5_blocks(N, TC) : 0, stack != 0);
@@ -1299,7 +1443,7 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
         if (a.det_groups) *a.det_groups = tch.groups;
     }
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
-    kern<<<grid, dim3(TC, T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
+    kern<<<grid, dim3(cols_tx(TC, ENG), T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
                                                   ctx.err_flag.as<int>(), a.p_row, det, stack);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
@@ -1353,6 +1497,13 @@ bool cols_ct_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int
     // TC x N/8 threads per CTA, at most 1024
     if (tc * (N / 8) > 1024 || a.ny % tc) return false;
     if (ctx.tma && a.mode != 2) {
+        // column pairs (engine 5): tiles of 8 columns at 512 and 16 at 256, where the column tile is automatic or that
+        if constexpr (N == 512 || N == 256) {
+            constexpr int TP = (N == 512) ? 8 : 16;
+            if (ctx.paired && (ctx.col_tile == 0 || ctx.col_tile == TP) && a.ny % TP == 0 &&
+                launch_cols_tma<N, TP, 5>(ctx, p, a, count))
+                return true;
+        }
         switch (tc) {
             case 2: if (launch_cols_tma<N, 2>(ctx, p, a, count)) return true; break;
             case 4: if (launch_cols_tma<N, 4>(ctx, p, a, count)) return true; break;
@@ -1641,6 +1792,7 @@ int propagate_fused(Context& ctx, PotentialImpl& pot, double energy, double tx, 
     key_append(key, kspace_last);
     key_append(key, ctx.form);
     key_append(key, ctx.col_tile);
+    key_append(key, ctx.paired);
     key_append(key, ctx.tma);
     key_append(key, ctx.tcgen05);
     key_append(key, ctx.composite);

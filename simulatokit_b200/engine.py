@@ -26,13 +26,15 @@ class ExecutionOptions:
     epilogue_detect: sum the channel detectors inside the last column pass (TMA passes) instead of separate kernels.
     composite: at grid sides 3 or 5 times a power of two (384, 640, 768, 1536) the fused passes transform each line as
     register-resident power-of-two transforms of its decimated sub-lines; False keeps the shared-memory Stockham
-    engine."""
+    engine. paired: at grid sides 512 and 256 the fused column pass takes tiles of 8 or 16 columns, one thread per
+    pair of adjacent columns (64- and 128-byte row segments in HBM), where col_tile is 0 or that width; False keeps
+    one column a thread."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 
     def __init__(self, form: str = "fused", batch: int = 0, batch_bytes: int = 1 << 30, graphs: bool = True,
                  col_tile: int = 0, tma: bool = True, autotune: bool = False, tcgen05: int = 2,
-                 epilogue_detect: bool = True, composite: bool = True):
+                 epilogue_detect: bool = True, composite: bool = True, paired: bool = True):
         if form not in self.FORMS:
             raise L.InvalidArgument(L.SIMK_ERR_INVALID, f"unknown form {form!r}")
         self.form = form
@@ -45,6 +47,7 @@ class ExecutionOptions:
         self.tcgen05 = int(tcgen05)  # 2: six stacked products a stage, 1 / True: twelve of N = 32, 0: mma.sync
         self.epilogue_detect = bool(epilogue_detect)
         self.composite = bool(composite)
+        self.paired = bool(paired)
 
     @staticmethod
     def standard() -> "ExecutionOptions":
@@ -92,6 +95,7 @@ class Engine:
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_TCGEN05, int(o.tcgen05)))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_EPILOGUE_DETECT, 1 if o.epilogue_detect else 0))
         L.check(self.lib.simk_context_set_option(self.handle, L.OPT_COMPOSITE, 1 if o.composite else 0))
+        L.check(self.lib.simk_context_set_option(self.handle, L.OPT_PAIRED, 1 if o.paired else 0))
 
     def set_stream(self, stream_ptr: int | None):
         L.check(self.lib.simk_context_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
