@@ -10,7 +10,8 @@ Timed region (`value`): `simk_scan_device` with the potential's transmissions al
 detector outputs on the device; K scans between CUDA events on the library's stream (torch's current stream),
 synchronised and barriered on both sides, max over ranks. The waves of a batch (up to 1 GiB) exceed L2 (126 MB), so
 no flush is needed between steps. `e2e`: the public `STEM.scan` call from host arrays (structure -> potential built on
-the device -> scan -> detector images back to the host), wall-clocked per call.
+the device -> scan -> detector images back to the host), wall-clocked per call, the median of --e2e-steps calls (5)
+after one warm-up call.
 
 `forms`: after the headline, one timed scan of each form (plain float32, fused float32, bf16x3 split-BF16 tensor-core
 stages) on the same stream, and, with the CPU leg, each form's relative L2 error per detector image against the float64
@@ -763,7 +764,7 @@ def main():
     ap.add_argument("--no-tma", action="store_true")
     ap.add_argument("--autotune", action="store_true", help="time column tile, TMA passes and batch on first use")
     ap.add_argument("--cpu-positions", type=int, default=32)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison after the headline")
     ap.add_argument("--no-other-configs", action="store_true",
