@@ -687,7 +687,8 @@ __global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols
                                                                float2* __restrict__ psi, float pscale, int ny,
                                                                int count, const float2* __restrict__ tw, int* err,
                                                                const int* __restrict__ p_row, const DetectArgs det,
-                                                               int tc5_stack) {
+                                                               int tc5_stack, const float2* __restrict__ rx,
+                                                               const float2* __restrict__ ry) {
     extern __shared__ __align__(128) unsigned char smem_tma[];
     constexpr int T = N / 8;
     constexpr int BOXH = tma_box_rows(N);
@@ -732,6 +733,10 @@ __global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
         float2* dst = stages + s * SST;
         const int prow = p_row ? p_row[b] * N : 0;  // job tables: this wave's propagator among the stacked ones
+        if constexpr (MODE == 2) {
+            mbar_arrive_expect_tx(&full[s], 0);  // probes: no wave to load, the phase completes at once
+            return;
+        }
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
 #pragma unroll
         for (int k = 0; k < NBOX; ++k) {
@@ -743,7 +748,7 @@ __global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols
     [[maybe_unused]] auto issue_p = [&](unsigned tile) {
         const int b = (int)(tile / tiles_per_wave);
         const int iy0 = (int)(tile - (unsigned)b * tiles_per_wave) * TC;
-        const int prow = p_row ? p_row[b] * N : 0;
+        const int prow = (MODE != 2 && p_row) ? p_row[b] * N : 0;
         mbar_arrive_expect_tx(&pfull, (uint32_t)TILE * sizeof(float2));
 #pragma unroll
         for (int k = 0; k < NBOX; ++k) tma_load_2d(ptile + k * BOXH * TC, &pmap, &pfull, 2 * iy0, prow + k * BOXH);
@@ -798,32 +803,48 @@ __global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols
             store_src = buf;
         } else if constexpr (ENG == 5) {
             // column pairs: thread (c, t) holds columns 2c, 2c + 1 of rows t + T i (one 16-byte access per row)
+            static_assert(TX == 4 || TX == 8, "column pairs: four or eight pairs a tile");
             float4* const tile4 = reinterpret_cast<float4*>(buf);
             const float4* const p4 = reinterpret_cast<const float4*>(pbuf);
-            float2 v0[8], v1[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float4 x = tile4[(t + T * i) * TX + c];
-                v0[i] = make_float2(x.x, x.y);
-                v1[i] = make_float2(x.z, x.w);
-            }
-            __syncthreads();  // the wave tile has been read: it becomes the pairs' exchange regions
-            static_assert(TX == 4 || TX == 8, "column pairs: four or eight pairs a tile");
             float4* const region = tile4 + c * N;
             // the slot XOR that spreads a quarter warp (two t and four pairs, or one t and eight) over the bank groups
             const int xc = (TX == 4) ? 2 * c : c;
-            ct2_fft_from<N, 0, -1>(v0, v1, t, eng, region, xc, [] {});
+            // behind the first barrier of the transform that follows the last read of the P buffer, every thread has
+            // read it: the next tile's P (or spectrum) may come
+            auto next_p = [&] {
+                if (tid == 0 && !abort_flag && next < ntiles) issue_p(next);
+            };
+            float2 v0[8], v1[8];
+            if constexpr (MODE == 2) {
+                // probes: the spectrum tile (in the P buffer) times the shift ramps r_x[ix] r_y[iy] of wave b, then the
+                // inverse transform; nothing is read from the stage
+                const int col = iy + c;  // iy - c + 2 c: the pair's first column
+                const float2 ry0 = __ldg(ry + (size_t)b * ny + col), ry1 = __ldg(ry + (size_t)b * ny + col + 1);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float4 pp = p4[(t + T * i) * TX + c];
-                v0[i] = cmul(v0[i], make_float2(pp.x, pp.y)) * pscale;
-                v1[i] = cmul(v1[i], make_float2(pp.z, pp.w)) * pscale;
-            }
-            if constexpr (MODE == 0) {
-                // behind the inverse transform's first barrier every thread has multiplied: the next tile's P may come
-                ct2_fft_from<N, 0, +1>(v0, v1, t, eng, region, xc, [&] {
-                    if (tid == 0 && !abort_flag && next < ntiles) issue_p(next);
-                });
+                for (int i = 0; i < 8; ++i) {
+                    const int ix = (int)t + T * i;
+                    const float4 sp = p4[ix * TX + c];
+                    const float2 r = __ldg(rx + (size_t)b * N + ix);
+                    v0[i] = cmul(cmul(make_float2(sp.x, sp.y), r), ry0);
+                    v1[i] = cmul(cmul(make_float2(sp.z, sp.w), r), ry1);
+                }
+                ct2_fft_from<N, 0, +1>(v0, v1, t, eng, region, xc, next_p);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float4 x = tile4[(t + T * i) * TX + c];
+                    v0[i] = make_float2(x.x, x.y);
+                    v1[i] = make_float2(x.z, x.w);
+                }
+                __syncthreads();  // the wave tile has been read: it becomes the pairs' exchange regions
+                ct2_fft_from<N, 0, -1>(v0, v1, t, eng, region, xc, [] {});
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float4 pp = p4[(t + T * i) * TX + c];
+                    v0[i] = cmul(v0[i], make_float2(pp.x, pp.y)) * pscale;
+                    v1[i] = cmul(v1[i], make_float2(pp.z, pp.w)) * pscale;
+                }
+                if constexpr (MODE == 0) ct2_fft_from<N, 0, +1>(v0, v1, t, eng, region, xc, next_p);
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i)
@@ -922,7 +943,7 @@ __global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols
             for (int k = 0; k < NBOX; ++k) tma_store_2d(&map, store_src + k * BOXH * TC, 2 * iy0, b * N + k * BOXH);
             bulk_commit();
         }
-        if constexpr (PSEP && MODE != 0) {
+        if constexpr (PSEP && MODE != 0 && MODE != 2) {
             // without an inverse transform the P tile is free from the barrier above on
             if (tid == 0 && !abort_flag && next < ntiles) issue_p(next);
         }
@@ -1427,8 +1448,11 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     if (blocks_per_sm <= 0) return false;
     ensure_err_flag(ctx);
     const CUtensorMap map = encode_tensor_map_2d(a.psi, 2ULL * a.ny, (unsigned long long)count * N, 2 * TC, BOXH);
-    const CUtensorMap pmap = encode_tensor_map_2d(const_cast<float2*>(a.P), 2ULL * a.ny,
-                                                  (unsigned long long)std::max(1, a.p_blocks) * N, 2 * TC, BOXH);
+    // the P tiles, or for the probes (MODE 2) the spectrum's
+    const CUtensorMap pmap =
+        MODE == 2 ? encode_tensor_map_2d(const_cast<float2*>(a.spectrum), 2ULL * a.ny, (unsigned long long)N, 2 * TC, BOXH)
+                  : encode_tensor_map_2d(const_cast<float2*>(a.P), 2ULL * a.ny,
+                                         (unsigned long long)std::max(1, a.p_blocks) * N, 2 * TC, BOXH);
     const long long ntiles = (long long)count * (a.ny / TC);
     if (ntiles >= (1LL << 31)) return false;
     DetectArgs det{};
@@ -1444,7 +1468,7 @@ bool launch_cols_tma_m(Context& ctx, const RegPlan& p, const ColArgs& a, int cou
     }
     const int grid = (int)std::min<long long>(ntiles, (long long)blocks_per_sm * ctx.sm_count);
     kern<<<grid, dim3(cols_tx(TC, ENG), T), smem, ctx.stream>>>(map, pmap, a.psi, a.pscale, a.ny, count, p.tw,
-                                                  ctx.err_flag.as<int>(), a.p_row, det, stack);
+                                                  ctx.err_flag.as<int>(), a.p_row, det, stack, a.rx, a.ry);
     SIMK_CUDA(cudaGetLastError());
     ++ctx.launches;
     return true;
@@ -1457,6 +1481,9 @@ bool launch_cols_tma(Context& ctx, const RegPlan& p, const ColArgs& a, int count
     if (a.mode == 0) return launch_cols_tma_m<N, TC, 0, ENG>(ctx, p, a, count);
     if (a.mode == 1) return launch_cols_tma_m<N, TC, 1, ENG>(ctx, p, a, count);
     if (a.mode == 3) return launch_cols_tma_m<N, TC, 3, ENG>(ctx, p, a, count);
+    if constexpr (ENG == 5) {
+        if (a.mode == 2) return launch_cols_tma_m<N, TC, 2, ENG>(ctx, p, a, count);  // probes from their spectrum
+    }
     return false;
 }
 
@@ -1496,14 +1523,15 @@ template <int N>
 bool cols_ct_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
     // TC x N/8 threads per CTA, at most 1024
     if (tc * (N / 8) > 1024 || a.ny % tc) return false;
+    // column pairs (engine 5, every mode including the probes' generation): tiles of 8 columns at 512 and 16 at 256,
+    // where the column tile is automatic or that
+    if constexpr (N == 512 || N == 256) {
+        constexpr int TP = (N == 512) ? 8 : 16;
+        if (ctx.tma && ctx.paired && (ctx.col_tile == 0 || ctx.col_tile == TP) && a.ny % TP == 0 &&
+            launch_cols_tma<N, TP, 5>(ctx, p, a, count))
+            return true;
+    }
     if (ctx.tma && a.mode != 2) {
-        // column pairs (engine 5): tiles of 8 columns at 512 and 16 at 256, where the column tile is automatic or that
-        if constexpr (N == 512 || N == 256) {
-            constexpr int TP = (N == 512) ? 8 : 16;
-            if (ctx.paired && (ctx.col_tile == 0 || ctx.col_tile == TP) && a.ny % TP == 0 &&
-                launch_cols_tma<N, TP, 5>(ctx, p, a, count))
-                return true;
-        }
         switch (tc) {
             case 2: if (launch_cols_tma<N, 2>(ctx, p, a, count)) return true; break;
             case 4: if (launch_cols_tma<N, 4>(ctx, p, a, count)) return true; break;

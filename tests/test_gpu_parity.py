@@ -303,3 +303,50 @@ def test_composite_engine_scan(engine, n, col_tile):
         e_o, e_e = O.rel_l2(a.values, r.ravel()), O.rel_l2(a.values, b.values)
         print(f"{n}^2 tile {col_tile}: composite vs float64 {e_o:.2e}, vs shared-memory engine {e_e:.2e}")
         assert e_o <= to and e_e <= te
+
+
+@pytest.mark.parametrize("n", [512, 256])
+def test_column_pairs(engine, n):
+    """The column pass on column pairs (8-column tiles at 512, 16 at 256, one thread per pair of adjacent columns: the
+    slices' passes, the probes' generation from their spectrum and the last pass with the detector epilogue or the
+    k-space store) against the one-column-a-thread pass and the float64 oracle: a plane-wave exit wave (<= 1e-5 against
+    float64; the two passes run the same butterflies and twiddles per column, but the compiler's fused multiply-adds
+    may differ, so they agree to float32 rounding, <= 1e-6) and a probe scan with annular, centre-of-mass and
+    pixelated detectors (<= 1e-4 / 1e-3 against float64, <= 1e-6 between the passes)."""
+    s = O.srtio3_cell().repeated(2, 2, 2)
+    st = sk.AtomicStructure(s.box, s.numbers, s.positions)
+    op = O.Potential.from_structure(s, n, n, slice_thickness=1.9525)
+    og = op.grid
+    ts = [O.transmission(v, 200e3, og) for v in op.build()]
+    ref = O.multislice(O.plane_wave(og), ts, op.thicknesses, 200e3, og)[-1]
+    pot = sk.Potential(st, n, n, slice_thickness=1.9525)
+    waves = {}
+    for paired in (True, False):
+        opts = sk.ExecutionOptions(form="fused", paired=paired)
+        waves[paired] = sk.Multislice.run(sk.Waves.plane_wave(sk.ElectronBeam(200e3), pot.grid), pot, options=opts,
+                                          engine=engine)[-1].field
+    e_ref, e_pair = O.rel_l2(waves[True], ref), O.rel_l2(waves[True], waves[False])
+    print(f"{n}^2 exit wave: pairs vs float64 {e_ref:.2e}, vs single columns {e_pair:.2e}, "
+          f"identical {np.array_equal(waves[True], waves[False])}")
+    assert e_ref <= 1e-5 and e_pair <= 1e-6
+    probe = sk.Probe(sk.ElectronBeam(200e3), pot.grid, sk.Aperture(20.0))
+    scan = sk.GridScan((1.0, 1.0), (4.0, 4.0), 3, 3)
+    dets = [sk.AnnularDetector(0, 20), sk.AnnularDetector(50, 120), sk.CenterOfMassDetector("cutoff", "mrad")]
+    pix = [sk.PixelatedDetector("cutoff")]
+    out = {}
+    for paired in (True, False):
+        opts = sk.ExecutionOptions(form="fused", paired=paired)
+        out[paired] = (sk.STEM.scan(probe, [pot], scan, dets, options=opts, engine=engine),
+                       sk.STEM.scan(probe, [pot], scan, dets + pix, options=opts, engine=engine))
+    ores = O.stem_scan(O.ProbeSpec(200e3, 20.0), [(og, op.build(), op.thicknesses)], scan.positions,
+                       [O.DetectorSpec("annular", {"inner": 0, "outer": 20}),
+                        O.DetectorSpec("annular", {"inner": 50, "outer": 120}),
+                        O.DetectorSpec("com", {"mode": "cutoff", "units": "mrad"})])
+    for k in range(2):  # channel detectors in the epilogue; with a pixelated detector, from the stored k-space waves
+        for a, b, r, to in zip(out[True][k], out[False][k], ores, (1e-4, 1e-4, 1e-3)):
+            e_o, e_e = O.rel_l2(a.values, np.asarray(r).ravel()), O.rel_l2(a.values, b.values)
+            print(f"{n}^2 scan {k}: pairs vs float64 {e_o:.2e}, vs single columns {e_e:.2e}")
+            assert e_o <= to and e_e <= 1e-6
+    e_pix = O.rel_l2(out[True][1][-1].values, out[False][1][-1].values)
+    print(f"{n}^2 pixelated: pairs vs single columns {e_pix:.2e}")
+    assert e_pix <= 1e-6
