@@ -46,9 +46,9 @@ extern "C" {
 #define SIMK_OPT_TMA 6          /* TMA-pipelined persistent column pass where the grid allows it (default 1) */
 #define SIMK_OPT_GRAPHS_CACHED 7 /* read-only: slice loops held as instantiated CUDA graphs */
 /* On the first fused scan of a grid shape and form, time one slice step of the actual transmission and propagator
- * for each column tile (2, 4, 8), with and without the TMA passes, then for batch sizes up to what half of the free
- * device memory holds, and use the fastest wherever SIMK_OPT_COL_TILE / SIMK_OPT_BATCH are 0 (automatic) and TMA is
- * allowed. The choice is kept per (grid, form) in the context. Default 0 (off). */
+ * for each column tile (2, 4, 8, and 16 at 256 x 256 with SIMK_OPT_PAIRED), with and without the TMA passes, then for
+ * batch sizes up to what half of the free device memory holds, and use the fastest wherever SIMK_OPT_COL_TILE /
+ * SIMK_OPT_BATCH are 0 (automatic) and TMA is allowed. The choice is kept per (grid, form) in the context. Default 0 (off). */
 #define SIMK_OPT_AUTOTUNE 8
 #define SIMK_OPT_TUNED_COL_TILE 9 /* read-only: the last tuning's choice (-1 before any) */
 #define SIMK_OPT_TUNED_TMA 10

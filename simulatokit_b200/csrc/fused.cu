@@ -2031,8 +2031,10 @@ Context::Tuned autotune(Context& ctx, PotentialImpl& pot, double energy, double 
                 if (tma && !save_tma) continue;
                 if (!tma && ctx.form == SIMK_FORM_BF16X3) continue;  // the tensor-core form runs on the TMA passes only
                 if (!tma && eng == 0 && ctx.form == SIMK_FORM_FUSED) continue;  // the engines differ on TMA passes only
-                for (int tc : {2, 4, 8}) {
+                for (int tc : {2, 4, 8, 16}) {
                     if (g.ny % tc || tc * (g.nx / 8) > 1024) continue;
+                    // 16 columns only where the column pairs take them (256^2)
+                    if (tc == 16 && !(ctx.paired && g.nx == 256 && ctx.form == SIMK_FORM_FUSED && tma)) continue;
                     ctx.tma = tma;
                     ctx.col_tile = tc;
                     const double t = time_per_wave(b0);

@@ -28,7 +28,8 @@ def test_autotune_choice_and_results(engine, form, n):
                              engine=engine)
     t = engine.tuned()
     print(form, n, t)
-    assert t["col_tile"] in (2, 4, 8) and t["tma"] in (0, 1) and 1 <= t["batch"] <= 1024
+    assert t["col_tile"] in ((2, 4, 8, 16) if (form, n) == ("fused", 256) else (2, 4, 8))
+    assert t["tma"] in (0, 1) and 1 <= t["batch"] <= 1024
     # the engine: composite or shared-memory at 768 (fused), a tcgen05 product order or mma.sync at 256 (bf16x3)
     assert t["engine"] in ((0, 1) if (form, n) == ("fused", 768) else (0, 1, 2) if form == "bf16x3" else (-1,))
     kw = {}
