@@ -596,7 +596,8 @@ __device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool n
 // Engines: 0 register-resident float32 Cooley-Tukey passes (powers of two); 1 radix-16 stages as mma.sync products of
 // split-BF16 operands on a shared-memory tile (tcfft.cuh, the bf16x3 form); 2 float32 shared-memory Stockham
 // (ccfft.cuh); 3 radix-16 stages as tcgen05.mma products (tc5fft.cuh, the bf16x3 form at 256 and 512); 4 the composite
-// register engine (lengths 3 or 5 times a power of two: R sub-lines of engine 0).
+// register engine (lengths 3 or 5 times a power of two: R sub-lines of engine 0); 5 engine 0 on column pairs (8- or
+// 16-column tiles, two adjacent columns a thread; MODE 2 there generates the probes from their spectrum).
 // Height of the column pass's TMA boxes: the largest divisor of N that is at most 256 (the box limit).
 constexpr int tma_box_rows(int n) {
     for (int h = 256; h > 1; --h)
@@ -707,7 +708,7 @@ __global__ void __launch_bounds__(cols_tx(TC, ENG) * (N / 8), tc_min_blocks(cols
     __shared__ __align__(8) uint64_t mma_bar;
     __shared__ double red5[PSEP && MODE == 3 ? TX * T / 32 * 64 : 1];  // engine 5's detector sums (C <= 64)
     float2* stages = reinterpret_cast<float2*>(smem_tma);
-    [[maybe_unused]] float2* const ptile = stages + 2 * SST;  // engine 5's P tile
+    [[maybe_unused]] float2* const ptile = stages + 2 * SST;  // engine 5's P tile (the spectrum's in MODE 2)
     const int c = threadIdx.x;
     const unsigned t = threadIdx.y;
     const int tid = (int)t * TX + c;
