@@ -592,7 +592,8 @@ __device__ __forceinline__ void stage_wait(uint64_t* full, int s, int it, bool n
     }
 }
 
-// columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each.
+// columns: tile = (wave b, TC columns from iy0); a stage holds the wave tile and the P tile, N x TC each (engine 5:
+// the wave tile only, beside one P buffer).
 // Engines: 0 register-resident float32 Cooley-Tukey passes (powers of two); 1 radix-16 stages as mma.sync products of
 // split-BF16 operands on a shared-memory tile (tcfft.cuh, the bf16x3 form); 2 float32 shared-memory Stockham
 // (ccfft.cuh); 3 radix-16 stages as tcgen05.mma products (tc5fft.cuh, the bf16x3 form at 256 and 512); 4 the composite
