@@ -2230,7 +2230,7 @@ struct TableCache {
 std::string table_key(const Context& ctx, const std::vector<JobSpec>& jobs) {
     std::string k;
     auto add = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
-    const int opts[] = {ctx.form, ctx.tma, ctx.col_tile, ctx.composite, ctx.tcgen05};
+    const int opts[] = {ctx.form, ctx.tma, ctx.col_tile, ctx.composite, ctx.tcgen05, ctx.paired};
     add(opts, sizeof(opts));
     for (const JobSpec& j : jobs) {
         const void* ids[] = {j.pot, j.pot->t.ptr};

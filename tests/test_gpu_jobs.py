@@ -32,11 +32,10 @@ def _cell(name):
     return {"srtio3": O.srtio3_cell, "silicon": O.silicon_cell, "al": O.al_fcc_cell}[name]()
 
 
-@pytest.fixture(scope="module")
-def table():
+def _build(jobs):
     t = sk.JobTable()
     refs = []
-    for name, rep, (nx, ny), dz, energy, probe in JOBS:
+    for name, rep, (nx, ny), dz, energy, probe in jobs:
         s = _cell(name).repeated(*rep)
         pot = sk.Potential(sk.AtomicStructure(s.box, s.numbers, s.positions), nx, ny, slice_thickness=dz)
         op = O.Potential.from_structure(s, nx, ny, slice_thickness=dz)
@@ -53,6 +52,11 @@ def table():
         ex = O.multislice(psi0, ts, op.thicknesses, energy, og)[-1]
         refs.append((np.abs(ex) ** 2, len(op.thicknesses)))
     return t, refs
+
+
+@pytest.fixture(scope="module")
+def table():
+    return _build(JOBS)
 
 
 @pytest.mark.parametrize("form", ["fused", "plain"])
@@ -101,3 +105,21 @@ def test_job_table_refusals(engine):
         t.run(engine=engine)
     outs, done = sk.JobTable().run(engine=engine)
     assert outs == [] and len(done) == 0
+
+
+def test_job_table_column_pairs_512(engine):
+    """Jobs of one 512 x 512 shape with different energies, slice counts and incident waves: each wave reads its own
+    propagator tile in the column pairs' P buffer. Intensities against the float64 oracle (<= 1e-5 relative L2) and
+    against the one-column-a-thread passes (<= 1e-6)."""
+    jobs = [("srtio3", (2, 2, 2), (512, 512), 1.9525, 200e3, None),
+            ("srtio3", (2, 2, 3), (512, 512), 1.9525, 120e3, (20.0, 0.0)),
+            ("silicon", (2, 2, 1), (512, 512), 1.35775, 300e3, (25.0, -50.0))]
+    t, refs = _build(jobs)
+    outs = {}
+    for paired in (True, False):
+        outs[paired], done = t.run(options=sk.ExecutionOptions(form="fused", paired=paired), engine=engine)
+        assert np.all(done > 0)
+    for k, (a, b, (ref, _)) in enumerate(zip(outs[True], outs[False], refs)):
+        e_o, e_p = O.rel_l2(a, ref), O.rel_l2(a, b)
+        print(f"512 job {k}: pairs vs float64 {e_o:.2e}, vs single columns {e_p:.2e}")
+        assert e_o <= 1e-5 and e_p <= 1e-6, (k, e_o, e_p)
