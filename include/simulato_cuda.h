@@ -76,8 +76,8 @@ extern "C" {
  * register engine (each line as 3 or 5 register-resident power-of-two transforms of its decimated sub-lines); 0 = the
  * shared-memory Stockham engine. */
 #define SIMK_OPT_COMPOSITE 15
-/* The fused form's column passes at grid sides 512 and 256: 1 (default) = tiles of 8 (512) or 16 (256) columns, one
- * thread transforming the same rows of two adjacent columns, so that every global row segment is 64 or 128 bytes wide
+/* The fused form's column passes at grid sides 256, 512 and 1024: 1 (default) = tiles of 16 (256) or 8 columns, one
+ * thread transforming the same rows of two adjacent columns, so that every global row segment is 128 or 64 bytes wide
  * (the pass then moves its bytes at close to the device's copy rate), where SIMK_OPT_COL_TILE is 0 or that width;
  * 0 = one column a thread, SIMK_OPT_COL_TILE (default 4) columns a tile. */
 #define SIMK_OPT_PAIRED 20

@@ -1525,10 +1525,10 @@ template <int N>
 bool cols_ct_tc(Context& ctx, const RegPlan& p, const ColArgs& a, int count, int tc) {
     // TC x N/8 threads per CTA, at most 1024
     if (tc * (N / 8) > 1024 || a.ny % tc) return false;
-    // column pairs (engine 5, every mode including the probes' generation): tiles of 8 columns at 512 and 16 at 256,
-    // where the column tile is automatic or that
-    if constexpr (N == 512 || N == 256) {
-        constexpr int TP = (N == 512) ? 8 : 16;
+    // column pairs (engine 5, every mode including the probes' generation): tiles of 8 columns at 512 and 1024 (one
+    // 512-thread CTA an SM there) and 16 at 256, where the column tile is automatic or that
+    if constexpr (N == 512 || N == 256 || N == 1024) {
+        constexpr int TP = (N == 256) ? 16 : 8;
         if (ctx.tma && ctx.paired && (ctx.col_tile == 0 || ctx.col_tile == TP) && a.ny % TP == 0 &&
             launch_cols_tma<N, TP, 5>(ctx, p, a, count))
             return true;

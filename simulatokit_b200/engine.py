@@ -26,9 +26,9 @@ class ExecutionOptions:
     epilogue_detect: sum the channel detectors inside the last column pass (TMA passes) instead of separate kernels.
     composite: at grid sides 3 or 5 times a power of two (384, 640, 768, 1536) the fused passes transform each line as
     register-resident power-of-two transforms of its decimated sub-lines; False keeps the shared-memory Stockham
-    engine. paired: at grid sides 512 and 256 the fused column pass takes tiles of 8 or 16 columns, one thread per
-    pair of adjacent columns (64- and 128-byte row segments in HBM), where col_tile is 0 or that width; False keeps
-    one column a thread."""
+    engine. paired: at grid sides 512, 1024 and 256 the fused column pass takes tiles of 8 or 16 columns, one thread
+    per pair of adjacent columns (64- and 128-byte row segments in HBM), where col_tile is 0 or that width; False
+    keeps one column a thread."""
 
     FORMS = {"plain": L.FORM_PLAIN, "fused": L.FORM_FUSED, "bf16x3": L.FORM_BF16X3}
 

@@ -305,11 +305,11 @@ def test_composite_engine_scan(engine, n, col_tile):
         assert e_o <= to and e_e <= te
 
 
-@pytest.mark.parametrize("n", [512, 256])
+@pytest.mark.parametrize("n", [512, 256, 1024])
 def test_column_pairs(engine, n):
-    """The column pass on column pairs (8-column tiles at 512, 16 at 256, one thread per pair of adjacent columns: the
-    slices' passes, the probes' generation from their spectrum and the last pass with the detector epilogue or the
-    k-space store) against the one-column-a-thread pass and the float64 oracle: a plane-wave exit wave (<= 1e-5 against
+    """The column pass on column pairs (8-column tiles at 512 and 1024, 16 at 256, one thread per pair of adjacent
+    columns: the slices' passes, the probes' generation from their spectrum and the last pass with the detector epilogue
+    or the k-space store) against the one-column-a-thread pass and the float64 oracle: a plane-wave exit wave (<= 1e-5 against
     float64; the two passes run the same butterflies and twiddles per column, but the compiler's fused multiply-adds
     may differ, so they agree to float32 rounding, <= 1e-6) and a probe scan with annular, centre-of-mass and
     pixelated detectors (<= 1e-4 / 1e-3 against float64, <= 1e-6 between the passes)."""
