@@ -106,10 +106,13 @@ __global__ void k_exp_i_sigma_v(double2* T, const double* V, double sigma, long 
     }
 }
 
-__global__ void k_mul_antialias(double2* T, GridDev g) {
+// `count` fields of nx x ny, one after another.
+__global__ void k_mul_antialias(double2* T, GridDev g, int count) {
     const long long N = (long long)g.nx * g.ny;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-        const double a = antialias_at((int)(i / g.ny), (int)(i % g.ny), g);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N * count;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long k = i % N;
+        const double a = antialias_at((int)(k / g.ny), (int)(k % g.ny), g);
         T[i] = make_double2(T[i].x * a, T[i].y * a);
     }
 }
@@ -251,9 +254,16 @@ void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice,
     }
     SIMK_CUDA(cudaGetLastError());
     pot.V.alloc(std::max<long long>(1, S) * N * sizeof(double));
-    // the elements present in a slice are transformed together, up to `chunk` delta images (256 MiB) per batch
-    const int chunk = (int)std::max<long long>(1, std::min<long long>(E, (256LL << 20) / (N * (long long)sizeof(double2))));
-    DeviceBuffer spec(N * sizeof(double2)), delta((size_t)chunk * N * sizeof(double2));
+    // Slices go in groups: the delta images of a group's slices (the elements present in each, in increasing Z) are
+    // transformed as one batch of at most `chunk` images (64 MiB, at least one slice's worth up to 256 MiB), each
+    // slice's spectrum is accumulated from its own images in that order, and the group's spectra (at most `gmax`)
+    // are transformed back together. A slice whose images exceed the batch is a group of its own, its images
+    // transformed in turn. Every line transform and every pixel's sum is the same as one slice at a time.
+    const long long img = N * (long long)sizeof(double2);
+    const int gmax = (int)std::max<long long>(1, (64LL << 20) / img);
+    const int chunk = (int)std::max<long long>(
+        1, std::max<long long>(gmax, std::min<long long>(E, (256LL << 20) / img)));
+    DeviceBuffer spec((size_t)std::min(gmax, std::max(1, S)) * img), delta((size_t)chunk * img);
     DeviceBuffer d_elem((size_t)std::max(1, S * E) * sizeof(int));
     std::vector<int> present;  // per slice, the elements with atoms in it, in increasing Z; concatenated over slices
     std::vector<int> present_ptr(1, 0);
@@ -267,29 +277,59 @@ void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice,
                                   ctx.stream));
     const LinePlan& prow = ctx.plan(g.ny, 64);
     const LinePlan& pcol = ctx.plan(g.nx, 64);
-    for (int j = 0; j < S; ++j) {
-        k_zero_d2<<<blocks_for(N), 256, 0, ctx.stream>>>(spec.as<double2>(), N);
+    // delta image q (of the batch starting at q0) of slice j: its element's atoms scattered with their weights
+    auto scatter = [&](int j, int q_global, int q_local) {
+        const int e = present[q_global];
+        const long long a0 = group_ptr[j * E + e], a1 = group_ptr[j * E + e + 1];
+        k_scatter<<<blocks_for(a1 - a0), 256, 0, ctx.stream>>>(delta.as<double2>() + (long long)q_local * N,
+                                                                d_pix.as<int>() + a0, d_w.as<double>() + a0,
+                                                                (int)(a1 - a0));
         ++ctx.launches;
-        for (int q0 = present_ptr[j]; q0 < present_ptr[j + 1]; q0 += chunk) {
-            const int nq = std::min(chunk, present_ptr[j + 1] - q0);
-            k_zero_d2<<<blocks_for((long long)nq * N), 256, 0, ctx.stream>>>(delta.as<double2>(), (long long)nq * N);
-            ++ctx.launches;
-            for (int q = 0; q < nq; ++q) {
-                const int e = present[q0 + q];
-                const long long a0 = group_ptr[j * E + e], a1 = group_ptr[j * E + e + 1];
-                k_scatter<<<blocks_for(a1 - a0), 256, 0, ctx.stream>>>(delta.as<double2>() + (long long)q * N,
-                                                                        d_pix.as<int>() + a0, d_w.as<double>() + a0,
-                                                                        (int)(a1 - a0));
+    };
+    for (int j0 = 0; j0 < S;) {
+        int j1 = j0 + 1;
+        while (j1 < S && j1 - j0 < gmax && present_ptr[j1 + 1] - present_ptr[j0] <= chunk) ++j1;
+        const int G = j1 - j0;
+        const int imgs = present_ptr[j1] - present_ptr[j0];
+        k_zero_d2<<<blocks_for((long long)G * N), 256, 0, ctx.stream>>>(spec.as<double2>(), (long long)G * N);
+        ++ctx.launches;
+        if (imgs <= chunk) {
+            if (imgs > 0) {
+                k_zero_d2<<<blocks_for((long long)imgs * N), 256, 0, ctx.stream>>>(delta.as<double2>(),
+                                                                                   (long long)imgs * N);
+                ++ctx.launches;
+                for (int j = j0; j < j1; ++j)
+                    for (int q = present_ptr[j]; q < present_ptr[j + 1]; ++q) scatter(j, q, q - present_ptr[j0]);
+                fft2(prow, pcol, delta.ptr, g.nx, g.ny, imgs, -1, 1.0, ctx.stream, &ctx.launches);
+                for (int j = j0; j < j1; ++j) {
+                    const int nq = present_ptr[j + 1] - present_ptr[j];
+                    if (nq == 0) continue;
+                    k_accum_spectra<<<blocks_for(N), 256, 0, ctx.stream>>>(
+                        spec.as<double2>() + (long long)(j - j0) * N,
+                        delta.as<double2>() + (long long)(present_ptr[j] - present_ptr[j0]) * N, kern.as<double>(),
+                        d_elem.as<int>() + present_ptr[j], nq, N);
+                    ++ctx.launches;
+                }
+            }
+        } else {  // G == 1: the slice's images in batches of `chunk`
+            for (int q0 = present_ptr[j0]; q0 < present_ptr[j1]; q0 += chunk) {
+                const int nq = std::min(chunk, present_ptr[j1] - q0);
+                k_zero_d2<<<blocks_for((long long)nq * N), 256, 0, ctx.stream>>>(delta.as<double2>(),
+                                                                                 (long long)nq * N);
+                ++ctx.launches;
+                for (int q = 0; q < nq; ++q) scatter(j0, q0 + q, q);
+                fft2(prow, pcol, delta.ptr, g.nx, g.ny, nq, -1, 1.0, ctx.stream, &ctx.launches);
+                k_accum_spectra<<<blocks_for(N), 256, 0, ctx.stream>>>(spec.as<double2>(), delta.as<double2>(),
+                                                                        kern.as<double>(), d_elem.as<int>() + q0, nq,
+                                                                        N);
                 ++ctx.launches;
             }
-            fft2(prow, pcol, delta.ptr, g.nx, g.ny, nq, -1, 1.0, ctx.stream, &ctx.launches);
-            k_accum_spectra<<<blocks_for(N), 256, 0, ctx.stream>>>(spec.as<double2>(), delta.as<double2>(),
-                                                                    kern.as<double>(), d_elem.as<int>() + q0, nq, N);
-            ++ctx.launches;
         }
-        fft2(prow, pcol, spec.ptr, g.nx, g.ny, 1, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);
-        k_real_part<<<blocks_for(N), 256, 0, ctx.stream>>>(pot.V.as<double>() + j * N, spec.as<double2>(), N);
+        fft2(prow, pcol, spec.ptr, g.nx, g.ny, G, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);
+        k_real_part<<<blocks_for((long long)G * N), 256, 0, ctx.stream>>>(pot.V.as<double>() + (long long)j0 * N,
+                                                                          spec.as<double2>(), (long long)G * N);
         ++ctx.launches;
+        j0 = j1;
     }
     SIMK_CUDA(cudaGetLastError());
     SIMK_CUDA(cudaStreamSynchronize(ctx.stream));
@@ -302,18 +342,23 @@ void prepare_transmissions(Context& ctx, PotentialImpl& pot, double energy) {
     const long long N = g.count();
     const int S = pot.n_slices();
     pot.t.alloc(std::max(1, S) * N * sizeof(float2));
-    DeviceBuffer T(N * sizeof(double2));
+    // slices in batches of up to 64 MiB of float64 fields, each line transformed as it would be alone
+    const int C = (int)std::max<long long>(1, std::min<long long>(S, (64LL << 20) / (N * (long long)sizeof(double2))));
+    DeviceBuffer T((size_t)C * N * sizeof(double2));
     const LinePlan& prow = ctx.plan(g.ny, 64);
     const LinePlan& pcol = ctx.plan(g.nx, 64);
     const double sigma = interaction_parameter(energy);
-    for (int j = 0; j < S; ++j) {
-        k_exp_i_sigma_v<<<blocks_for(N), 256, 0, ctx.stream>>>(T.as<double2>(), pot.V.as<double>() + j * N, sigma, N);
+    for (int j0 = 0; j0 < S; j0 += C) {
+        const int c = std::min(C, S - j0);
+        const long long cn = (long long)c * N;
+        k_exp_i_sigma_v<<<blocks_for(cn), 256, 0, ctx.stream>>>(T.as<double2>(), pot.V.as<double>() + (long long)j0 * N,
+                                                                sigma, cn);
         ++ctx.launches;
-        fft2(prow, pcol, T.ptr, g.nx, g.ny, 1, -1, 1.0, ctx.stream, &ctx.launches);
-        k_mul_antialias<<<blocks_for(N), 256, 0, ctx.stream>>>(T.as<double2>(), grid_dev(g));
+        fft2(prow, pcol, T.ptr, g.nx, g.ny, c, -1, 1.0, ctx.stream, &ctx.launches);
+        k_mul_antialias<<<blocks_for(cn), 256, 0, ctx.stream>>>(T.as<double2>(), grid_dev(g), c);
         ++ctx.launches;
-        fft2(prow, pcol, T.ptr, g.nx, g.ny, 1, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);
-        k_to_float2<<<blocks_for(N), 256, 0, ctx.stream>>>(pot.t.as<float2>() + j * N, T.as<double2>(), N);
+        fft2(prow, pcol, T.ptr, g.nx, g.ny, c, +1, 1.0 / (double)N, ctx.stream, &ctx.launches);
+        k_to_float2<<<blocks_for(cn), 256, 0, ctx.stream>>>(pot.t.as<float2>() + (long long)j0 * N, T.as<double2>(), cn);
         ++ctx.launches;
     }
     SIMK_CUDA(cudaGetLastError());
