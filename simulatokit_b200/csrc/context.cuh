@@ -187,6 +187,10 @@ struct Context {
     // scan post-processing: the Gaussian passes' intermediate, their weights, the Poisson sampler's status word, the
     // gradient integration's two spectra and its minimum
     DeviceBuffer post_work, post_weights, post_flag, post_spectra, post_min;
+    // the potential builder's scratch, kept across builds (grown on demand): the atoms' merged pixels and weights, the
+    // elements' Lobato kernels and parameters, the present-element lists, the group's spectra and the delta images
+    // (which the transmissions reuse as their float64 fields)
+    DeviceBuffer pot_pix, pot_w, pot_kern, pot_ab, pot_elem, pot_spec, pot_delta;
     std::vector<DeviceBuffer> outputs;
     // per-scan set-up kept across calls: detector maps by (grid, energy, detectors), spectra by (grid, probe)
     std::map<std::string, std::unique_ptr<DetectorPlan>> detector_plans;

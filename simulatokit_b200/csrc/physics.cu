@@ -228,13 +228,18 @@ void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice,
         }
     }
     // device: kernels f/S per element (float64), then per slice sum_e FFT(deltas_e) f_e/S -> IFFT -> Re
-    DeviceBuffer d_pix(std::max<size_t>(1, pix.size() * sizeof(int))), d_w(std::max<size_t>(1, wts.size() * sizeof(double)));
+    DeviceBuffer& d_pix = ctx.pot_pix;
+    DeviceBuffer& d_w = ctx.pot_w;
+    d_pix.ensure(std::max<size_t>(1, pix.size() * sizeof(int)));
+    d_w.ensure(std::max<size_t>(1, wts.size() * sizeof(double)));
     if (!pix.empty()) {
         SIMK_CUDA(cudaMemcpyAsync(d_pix.ptr, pix.data(), pix.size() * sizeof(int), cudaMemcpyHostToDevice, ctx.stream));
         SIMK_CUDA(cudaMemcpyAsync(d_w.ptr, wts.data(), wts.size() * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
     }
-    DeviceBuffer kern(std::max<long long>(1, E) * N * sizeof(double));
-    DeviceBuffer ab(std::max(1, E) * 10 * sizeof(double));
+    DeviceBuffer& kern = ctx.pot_kern;
+    DeviceBuffer& ab = ctx.pot_ab;
+    kern.ensure(std::max<long long>(1, E) * N * sizeof(double));
+    ab.ensure(std::max(1, E) * 10 * sizeof(double));
     std::vector<double> hab(std::max(1, E) * 10);
     const double pi = (pi_choice == SIMK_PI_ABTEM_FLOAT32) ? (double)(float)M_PI : M_PI;
     const double pi2 = (pi_choice == SIMK_PI_ABTEM_FLOAT32) ? (double)(float)(M_PI * M_PI) : M_PI * M_PI;
@@ -263,8 +268,12 @@ void build_potential_from_atoms(Context& ctx, PotentialImpl& pot, int pi_choice,
     const int gmax = (int)std::max<long long>(1, (64LL << 20) / img);
     const int chunk = (int)std::max<long long>(
         1, std::max<long long>(gmax, std::min<long long>(E, (256LL << 20) / img)));
-    DeviceBuffer spec((size_t)std::min(gmax, std::max(1, S)) * img), delta((size_t)chunk * img);
-    DeviceBuffer d_elem((size_t)std::max(1, S * E) * sizeof(int));
+    DeviceBuffer& spec = ctx.pot_spec;
+    DeviceBuffer& delta = ctx.pot_delta;
+    DeviceBuffer& d_elem = ctx.pot_elem;
+    spec.ensure((size_t)std::min(gmax, std::max(1, S)) * img);
+    delta.ensure((size_t)chunk * img);
+    d_elem.ensure((size_t)std::max(1, S * E) * sizeof(int));
     std::vector<int> present;  // per slice, the elements with atoms in it, in increasing Z; concatenated over slices
     std::vector<int> present_ptr(1, 0);
     for (int j = 0; j < S; ++j) {
@@ -344,7 +353,8 @@ void prepare_transmissions(Context& ctx, PotentialImpl& pot, double energy) {
     pot.t.alloc(std::max(1, S) * N * sizeof(float2));
     // slices in batches of up to 64 MiB of float64 fields, each line transformed as it would be alone
     const int C = (int)std::max<long long>(1, std::min<long long>(S, (64LL << 20) / (N * (long long)sizeof(double2))));
-    DeviceBuffer T((size_t)C * N * sizeof(double2));
+    DeviceBuffer& T = ctx.pot_delta;  // the builder's delta-image scratch, grown if needed
+    T.ensure((size_t)C * N * sizeof(double2));
     const LinePlan& prow = ctx.plan(g.ny, 64);
     const LinePlan& pcol = ctx.plan(g.nx, 64);
     const double sigma = interaction_parameter(energy);
